@@ -1,0 +1,267 @@
+"""gisspa_b200: B200-native GisSPA 2D template-matching search.
+
+Thin ctypes binding of the C ABI in ``include/gisspa.h`` (the library
+``gisspa_b200/lib/libgisspa_b200.so``, built by ``gisspa_b200.build``).
+There is no CPU fallback: every call runs the CUDA kernels, and a missing
+library or GPU raises.
+
+Typical use mirrors the reference's driver (main.cu:1025-1269)::
+
+    ctx = Context(device=0)
+    ctx.set_templates(params, templates, first_ctf=(defocus, dfdiff, dfang))
+    picks = ctx.search(micrograph, ctf=(defocus, dfdiff, dfang))
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Sequence, Tuple
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libgisspa_b200.so")
+DRIVER_PATH = os.path.join(HERE, "lib", "gisspa_main")
+
+GS_OK = 0
+STATUS = {0: "ok", 1: "invalid argument", 2: "out of memory", 3: "CUDA error",
+          4: "invalid call order", 5: "unsupported input", 6: "device wait timed out",
+          7: "I/O error"}
+
+
+class GsParams(C.Structure):
+    _fields_ = [("apix", C.c_float), ("phi_step", C.c_float), ("kk", C.c_float),
+                ("energy", C.c_float), ("cs", C.c_float), ("highres", C.c_float),
+                ("lowres", C.c_float), ("d_m", C.c_float), ("thres", C.c_float),
+                ("window_size", C.c_int), ("overlap", C.c_int), ("phase_flip", C.c_int),
+                ("norm_type", C.c_int), ("invert", C.c_int), ("ampconst", C.c_float),
+                ("a", C.c_float), ("b", C.c_float), ("b2", C.c_float),
+                ("bfactor", C.c_float), ("bfactor2", C.c_float), ("bfactor3", C.c_float),
+                ("precision", C.c_int)]
+
+
+class GsCtf(C.Structure):
+    _fields_ = [("defocus", C.c_float), ("dfdiff", C.c_float), ("dfang", C.c_float)]
+
+
+class GsPick(C.Structure):
+    _fields_ = [("angle_index", C.c_int), ("phi", C.c_float), ("window_x", C.c_int),
+                ("window_y", C.c_int), ("template_index", C.c_int), ("center_x", C.c_float),
+                ("center_y", C.c_float), ("score", C.c_float)]
+
+
+class GsGeometry(C.Structure):
+    _fields_ = [("l", C.c_int), ("n_windows_x", C.c_int), ("n_windows_y", C.c_int),
+                ("n_angles", C.c_int), ("n_templates", C.c_int)]
+
+
+UNIT_DTYPE = np.dtype([("score", "<f4"), ("pos", "<i4"), ("peak", "<f4"), ("sigma", "<f4")])
+PICK_DTYPE = np.dtype([("angle_index", "<i4"), ("phi", "<f4"), ("window_x", "<i4"),
+                       ("window_y", "<i4"), ("template_index", "<i4"), ("center_x", "<f4"),
+                       ("center_y", "<f4"), ("score", "<f4")])
+
+# every entry point declared in include/gisspa.h
+EXPORTS = ("gs_status_string", "gs_version", "gs_params_default", "gs_ctx_create",
+           "gs_ctx_destroy", "gs_ctx_last_error", "gs_set_templates", "gs_get_geometry",
+           "gs_search", "gs_search_device", "gs_get_units", "gs_picks_free", "gs_get_timings")
+
+_lib_handle = None
+
+
+class GisspaError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__("%s (%d): %s" % (STATUS.get(status, "?"), status, msg))
+        self.status = status
+
+
+def load_library(path: Optional[str] = None) -> C.CDLL:
+    """Load the C-ABI library (raises if it has not been built)."""
+    global _lib_handle
+    if _lib_handle is not None and path is None:
+        return _lib_handle
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise FileNotFoundError("CUDA library not built: %s (run gisspa_b200.build)" % p)
+    lib = C.CDLL(p)
+    vp = C.c_void_p
+    lib.gs_status_string.restype = C.c_char_p
+    lib.gs_status_string.argtypes = [C.c_int]
+    lib.gs_version.restype = C.c_int
+    lib.gs_params_default.argtypes = [C.POINTER(GsParams)]
+    lib.gs_ctx_create.argtypes = [C.c_int, C.POINTER(vp)]
+    lib.gs_ctx_destroy.argtypes = [vp]
+    lib.gs_ctx_last_error.restype = C.c_char_p
+    lib.gs_ctx_last_error.argtypes = [vp]
+    lib.gs_set_templates.argtypes = [vp, C.POINTER(GsParams), C.POINTER(C.c_float), C.c_int,
+                                     C.c_int, C.c_int, C.POINTER(GsCtf)]
+    lib.gs_get_geometry.argtypes = [vp, C.c_int, C.c_int, C.POINTER(GsGeometry)]
+    lib.gs_search.argtypes = [vp, C.POINTER(C.c_float), C.c_int, C.c_int, C.POINTER(GsCtf),
+                              C.POINTER(C.POINTER(GsPick)), C.POINTER(C.c_size_t)]
+    lib.gs_search_device.argtypes = [vp, C.c_void_p, C.c_int, C.c_int, C.POINTER(GsCtf),
+                                     C.POINTER(C.POINTER(GsPick)), C.POINTER(C.c_size_t)]
+    lib.gs_get_units.argtypes = [vp, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]
+    lib.gs_picks_free.argtypes = [C.POINTER(GsPick)]
+    lib.gs_picks_free.restype = None
+    lib.gs_get_timings.argtypes = [vp, C.POINTER(C.c_float)]
+    if path is None:
+        _lib_handle = lib
+    return lib
+
+
+def default_params(**kw) -> GsParams:
+    """Reference defaults (DataReader.h:16-42) updated with ``kw``."""
+    lib = load_library()
+    p = GsParams()
+    lib.gs_params_default(C.byref(p))
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
+
+
+def params_from_config(cfg) -> GsParams:
+    """GsParams from a :class:`gisspa_b200.formats.Config`."""
+    return default_params(apix=cfg.apix, phi_step=cfg.phi_step, kk=cfg.kk, energy=cfg.energy,
+                          cs=cfg.cs, highres=cfg.highres, lowres=cfg.lowres, d_m=cfg.d_m,
+                          thres=cfg.thres, window_size=cfg.padding_size, overlap=cfg.overlap,
+                          phase_flip=cfg.phase_flip, norm_type=cfg.norm_type, invert=cfg.invert)
+
+
+def _ctf(c) -> GsCtf:
+    if isinstance(c, GsCtf):
+        return c
+    d, dd, da = c
+    return GsCtf(float(d), float(dd), float(da))
+
+
+class Context:
+    """One CUDA device + stream + the device buffers of a run (gs_ctx)."""
+
+    def __init__(self, device: int = 0):
+        self._lib = load_library()
+        self._h = C.c_void_p()
+        st = self._lib.gs_ctx_create(int(device), C.byref(self._h))
+        if st != GS_OK:
+            raise GisspaError(st, "gs_ctx_create(device=%d)" % device)
+
+    def _check(self, st: int, what: str) -> None:
+        if st != GS_OK:
+            msg = self._lib.gs_ctx_last_error(self._h).decode(errors="replace")
+            raise GisspaError(st, "%s: %s" % (what, msg))
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.gs_ctx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_templates(self, params: GsParams, templates: np.ndarray, first_ctf) -> None:
+        t = np.ascontiguousarray(templates, dtype=np.float32)
+        if t.ndim != 3:
+            raise ValueError("templates must be (N, ty, tx)")
+        n, ty, tx = t.shape
+        self._check(self._lib.gs_set_templates(self._h, C.byref(params),
+                                               t.ctypes.data_as(C.POINTER(C.c_float)), n, tx, ty,
+                                               C.byref(_ctf(first_ctf))), "gs_set_templates")
+        self._keep = t
+
+    def geometry(self, nx: int, ny: int) -> GsGeometry:
+        g = GsGeometry()
+        self._check(self._lib.gs_get_geometry(self._h, nx, ny, C.byref(g)), "gs_get_geometry")
+        return g
+
+    def _picks(self, ptr, n) -> np.ndarray:
+        out = np.zeros(n, dtype=PICK_DTYPE)
+        if n:
+            buf = (GsPick * n).from_address(C.addressof(ptr.contents))
+            out[:] = np.frombuffer(buf, dtype=PICK_DTYPE, count=n)
+            self._lib.gs_picks_free(ptr)
+        return out
+
+    def search(self, micrograph: np.ndarray, ctf) -> np.ndarray:
+        m = np.ascontiguousarray(micrograph, dtype=np.float32)
+        ny, nx = m.shape
+        ptr = C.POINTER(GsPick)()
+        n = C.c_size_t()
+        self._check(self._lib.gs_search(self._h, m.ctypes.data_as(C.POINTER(C.c_float)), nx, ny,
+                                        C.byref(_ctf(ctf)), C.byref(ptr), C.byref(n)), "gs_search")
+        return self._picks(ptr, n.value)
+
+    def search_device(self, dev_ptr: int, nx: int, ny: int, ctf) -> np.ndarray:
+        ptr = C.POINTER(GsPick)()
+        n = C.c_size_t()
+        self._check(self._lib.gs_search_device(self._h, C.c_void_p(int(dev_ptr)), nx, ny,
+                                               C.byref(_ctf(ctf)), C.byref(ptr), C.byref(n)),
+                    "gs_search_device")
+        return self._picks(ptr, n.value)
+
+    def units(self, shape: Optional[Tuple[int, int, int]] = None) -> np.ndarray:
+        """Dense (n_angles, n_windows, n_templates) table of the last search."""
+        n = C.c_size_t()
+        self._check(self._lib.gs_get_units(self._h, None, 0, C.byref(n)), "gs_get_units")
+        out = np.zeros(n.value, dtype=UNIT_DTYPE)
+        self._check(self._lib.gs_get_units(self._h, out.ctypes.data, n.value, C.byref(n)),
+                    "gs_get_units")
+        return out.reshape(shape) if shape is not None else out
+
+    def timings(self) -> np.ndarray:
+        t = (C.c_float * 4)()
+        self._check(self._lib.gs_get_timings(self._h, t), "gs_get_timings")
+        return np.array(t[:], dtype=np.float64)
+
+
+def run_config(config_path: str, device: Optional[int] = None, return_units: bool = False):
+    """Python mirror of the drop-in driver (main.cu:1025-1269 behaviour) over
+    the C ABI: returns the output lines (and optionally the dense per-unit
+    tables, one per micrograph).  Paths resolve relative to the current
+    directory, as in the reference."""
+    from . import formats
+    cfg = formats.read_config(config_path)
+    missing = formats.missing_required(cfg)
+    if missing:
+        raise ValueError("missing required keys: %s" % ", ".join(missing))
+    eul = formats.read_euler(cfg.eulerf)
+    n = eul.shape[0]
+    h = formats.read_mrc_header(cfg.temp2d)
+    whole = formats.read_mrc(cfg.temp2d, -1)
+    if whole.ndim == 2:
+        whole = whole[None]
+    stack = np.stack([whole[J] if J < whole.shape[0] else whole[0] for J in range(n)])
+    first = formats.read_lst_entry(cfg.inlst, cfg.first)
+    if first is None:
+        raise IOError("entry %d of %s not found" % (cfg.first, cfg.inlst))
+    params = params_from_config(cfg)
+    lines = []
+    tables = []
+    with Context(cfg.device_id if device is None else device) as ctx:
+        ctx.set_templates(params, stack, (first.defocus, first.dfdiff, first.dfang))
+        for m in range(cfg.first, cfg.last):
+            ent = formats.read_lst_entry(cfg.inlst, m)
+            if ent is None:
+                raise IOError("entry %d of %s not found" % (m, cfg.inlst))
+            img = formats.read_mrc(ent.path, ent.nn)
+            if img.ndim == 3:
+                img = img[0]
+            picks = ctx.search(img, (ent.defocus, ent.dfdiff, ent.dfang))
+            for pk in picks:
+                J = int(pk["template_index"])
+                lines.append(formats.format_pick_line(
+                    ent.nn, ent.path, ent.defocus, ent.dfdiff, ent.dfang, float(eul[J, 0]),
+                    float(eul[J, 1]), float(pk["phi"]), float(pk["center_x"]),
+                    float(pk["center_y"]), float(pk["score"])))
+            if return_units:
+                g = ctx.geometry(img.shape[1], img.shape[0])
+                tables.append(ctx.units((g.n_angles, g.n_windows_x * g.n_windows_y, g.n_templates)))
+    return (lines, tables) if return_units else lines

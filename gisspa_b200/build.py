@@ -1,0 +1,91 @@
+"""Build recipe: nvcc for sm_100a, in-tree outputs under gisspa_b200/lib/.
+
+    python -m gisspa_b200.build            # library + drop-in driver
+    python -m gisspa_b200.build --force
+
+Outputs
+  gisspa_b200/lib/libgisspa_b200.so   C ABI of include/gisspa.h (CUDA kernels)
+  gisspa_b200/lib/gisspa_main         drop-in CLI for the reference's ./main
+"""
+from __future__ import annotations
+
+import argparse
+import glob
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIBDIR = os.path.join(HERE, "lib")
+INCLUDE = os.path.join(ROOT, "include")
+LIB = os.path.join(LIBDIR, "libgisspa_b200.so")
+DRIVER = os.path.join(LIBDIR, "gisspa_main")
+
+NVCC = os.environ.get("NVCC", "nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
+
+
+def _newer(target: str, sources) -> bool:
+    if not os.path.exists(target):
+        return False
+    t = os.path.getmtime(target)
+    return all(os.path.getmtime(s) <= t for s in sources)
+
+
+def _run(cmd, cwd=None) -> None:
+    print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True, cwd=cwd)
+
+
+def build_library(force: bool = False) -> str:
+    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cuh"))
+                  + [os.path.join(INCLUDE, "gisspa.h")])
+    if not force and _newer(LIB, srcs):
+        return LIB
+    os.makedirs(LIBDIR, exist_ok=True)
+    _run([NVCC] + NVCC_FLAGS + ARCH + ["-shared", "-I" + INCLUDE, "-o", LIB,
+                                       os.path.join(CSRC, "gisspa.cu")])
+    return LIB
+
+
+def build_driver(force: bool = False) -> str:
+    dsrc = sorted(glob.glob(os.path.join(CSRC, "driver", "*.cpp")))
+    deps = dsrc + glob.glob(os.path.join(CSRC, "driver", "*.hpp")) + [LIB, os.path.join(INCLUDE, "gisspa.h")]
+    if not force and _newer(DRIVER, deps):
+        return DRIVER
+    _run(["g++", "-O2", "-std=c++17", "-Wall", "-I" + INCLUDE] + dsrc +
+         ["-L" + LIBDIR, "-lgisspa_b200", "-Wl,-rpath,$ORIGIN", "-o", DRIVER])
+    return DRIVER
+
+
+def build_reference_checker() -> bool:
+    """Compile the reference's own sources into oracle/_ref (test
+    infrastructure) when they are present on this machine."""
+    ref = os.environ.get("GISSPA_REFERENCE", "/root/reference")
+    if not os.path.isdir(ref):
+        return False
+    _run(["make", "-C", os.path.join(ROOT, "oracle"), "ref", "REF=" + ref])
+    return True
+
+
+def build_all(force: bool = False, reference: bool = True) -> None:
+    build_library(force)
+    build_driver(force)
+    if reference:
+        build_reference_checker()
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--no-reference", action="store_true")
+    a = ap.parse_args()
+    build_all(a.force, not a.no_reference)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

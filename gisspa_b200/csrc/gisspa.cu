@@ -1,0 +1,658 @@
+// C-ABI implementation of the GisSPA B200 search (include/gisspa.h).
+//
+// Host orchestration of the kernels in kernels.cuh / fft.cuh.  One context
+// = one device + one stream + the device buffers of the run.  The flow of a
+// search follows the reference's main.cu:1149-1269 for norm_type 0:
+// micrograph preprocessing, window spectra, then for every in-plane angle the
+// template-pair spectra and, for every window, the fused correlation passes.
+#include "gisspa.h"
+#include "kernels.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+using namespace gs;
+
+namespace {
+
+struct FftPlan {
+    FftDesc d;
+    float2* tw = nullptr;
+};
+
+struct DBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+};
+
+}  // namespace
+
+struct gs_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    std::map<int, FftPlan> plans;
+    // templates
+    bool have_tmpl = false;
+    gs_params p{};
+    gs_ctf ctf0{};
+    int l = 0, ntmpl = 0, tx = 0, ty = 0;
+    DBuf tmpl;  // ntmpl x l x l float (real templates after preprocessing)
+    // per-search buffers
+    DBuf in, q, cimg, img, stats, ra, rb, off, win, wsum, winv;
+    DBuf tspec, scratch, pstats, coef, acc, units, picks, count;
+    // last search
+    int last_na = 0, last_nw = 0, last_nt = 0;
+    bool have_units = false;
+    float timings[4] = {0, 0, 0, 0};
+};
+
+namespace {
+
+int set_err(gs_ctx* c, int code, const char* fmt, ...) {
+    if (c) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        c->err = buf;
+    }
+    return code;
+}
+
+#define CK(expr)                                                                                       \
+    do {                                                                                               \
+        cudaError_t e_ = (expr);                                                                       \
+        if (e_ != cudaSuccess) return set_err(ctx, GS_ERR_CUDA, "%s: %s", #expr, cudaGetErrorString(e_)); \
+    } while (0)
+#define CKL() CK(cudaGetLastError())
+#define TRY(expr)                  \
+    do {                           \
+        int s_ = (expr);           \
+        if (s_ != GS_OK) return s_; \
+    } while (0)
+
+int ensure(gs_ctx* ctx, DBuf& b, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (b.cap >= bytes) return GS_OK;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+    cudaError_t e = cudaMalloc(&b.p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        b.p = nullptr;
+        return set_err(ctx, GS_ERR_OOM, "cudaMalloc(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
+    }
+    b.cap = bytes;
+    return GS_OK;
+}
+
+template <class T>
+T* P(DBuf& b) { return reinterpret_cast<T*>(b.p); }
+
+void free_buf(DBuf& b) {
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+}
+
+// Radix order: 8s while they divide, then 4, 2, 3, 5, then any other prime.
+int factorize(int n, int* radix) {
+    int ns = 0;
+    int m = n;
+    while (m % 8 == 0 && m > 1) { radix[ns++] = 8; m /= 8; }
+    while (m % 4 == 0) { radix[ns++] = 4; m /= 4; }
+    while (m % 2 == 0) { radix[ns++] = 2; m /= 2; }
+    for (int f : {3, 5}) while (m % f == 0) { radix[ns++] = f; m /= f; }
+    for (int f = 7; (long long)f * f <= m; f += 2)
+        while (m % f == 0) { radix[ns++] = f; m /= f; }
+    if (m > 1) radix[ns++] = m;
+    return ns;
+}
+
+int get_plan(gs_ctx* ctx, int n, FftPlan** out) {
+    auto it = ctx->plans.find(n);
+    if (it != ctx->plans.end()) {
+        *out = &it->second;
+        return GS_OK;
+    }
+    FftPlan pl;
+    pl.d.n = n;
+    pl.d.nst = factorize(n, pl.d.radix);
+    if (pl.d.nst > kFftMaxStages) return set_err(ctx, GS_ERR_UNSUPPORTED, "FFT length %d has too many factors", n);
+    for (int s = 0; s < pl.d.nst; ++s)
+        if (pl.d.radix[s] > 4096) return set_err(ctx, GS_ERR_UNSUPPORTED, "FFT length %d has prime factor %d", n, pl.d.radix[s]);
+    std::vector<float2> tw(n);
+    for (int k = 0; k < n; ++k) {
+        const double a = -2.0 * M_PI * (double)k / (double)n;
+        tw[k] = make_float2((float)cos(a), (float)sin(a));
+    }
+    CK(cudaMalloc(&pl.tw, sizeof(float2) * n));
+    CK(cudaMemcpy(pl.tw, tw.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
+    pl.d.tw = pl.tw;
+    auto res = ctx->plans.emplace(n, pl);
+    *out = &res.first->second;
+    return GS_OK;
+}
+
+constexpr int kFftThreads = 256;
+constexpr size_t kFftSmemBudget = 96 * 1024;
+constexpr size_t kMaxSmem = 227 * 1024;
+
+template <bool kInv, class IO>
+int run_fft(gs_ctx* ctx, int n, VecGeom g, int nimg, IO io, int max_tile = 16) {
+    FftPlan* pl = nullptr;
+    TRY(get_plan(ctx, n, &pl));
+    const size_t per = 2 * (size_t)(n + 1) * sizeof(float2);
+    size_t tile = std::max<size_t>(1, kFftSmemBudget / per);
+    if (per > kFftSmemBudget) tile = 1;
+    tile = std::min<size_t>(tile, (size_t)max_tile);
+    tile = std::min<size_t>(tile, (size_t)g.nvec);
+    const size_t smem = fft_smem_bytes(n, (int)tile);
+    if (smem > kMaxSmem) return set_err(ctx, GS_ERR_UNSUPPORTED, "FFT length %d exceeds shared memory", n);
+    if (nimg > 65535) return set_err(ctx, GS_ERR_UNSUPPORTED, "too many images in one FFT batch (%d)", nimg);
+    auto kern = fft_batched_kernel<kInv, IO>;
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid((unsigned)((g.nvec + tile - 1) / tile), (unsigned)nimg);
+    kern<<<grid, kFftThreads, smem, ctx->stream>>>(pl->d, g, (int)tile, io);
+    CKL();
+    return GS_OK;
+}
+
+// Row / column geometry of a batch of row-major h x w images (vectors of
+// length w for rows, h for columns).
+VecGeom rows_of(int w, int h) { return VecGeom{h, (long long)w, 1, (long long)w * h}; }
+VecGeom cols_of(int w, int h) { return VecGeom{w, 1, (long long)w, (long long)w * h}; }
+
+std::vector<int> window_offsets(int n, int l, int overlap) {
+    // main.cu:228-250 (interval > 0 is checked by the caller)
+    const int interval = l - overlap;
+    std::vector<int> offs{0};
+    int off = 0;
+    while (off + l < n) {
+        off += interval;
+        if (off + l >= n) off = n - l;
+        offs.push_back(off);
+    }
+    return offs;
+}
+
+std::vector<float> angle_list(float step) {
+    // main.cu:1232: float accumulation
+    std::vector<float> out;
+    for (float e = 0.0f; e < 360.0f; e += step) out.push_back(e);
+    return out;
+}
+
+float printed_phi(float e) {
+    float cur = 360.0f - e;  // main.cu:1254-1256
+    if (cur >= 360.0f) cur -= 360.0f;
+    return cur;
+}
+
+CtfDev make_ctf(const gs_params& p, const gs_ctf& c, int padding_for_ds, float* ds_out) {
+    // main.cu:150-155 + DataReader.cpp:375-385
+    CtfDev d;
+    const float defocus = -c.defocus;
+    d.apix = p.apix;
+    d.dfu = defocus + c.dfdiff;
+    d.dfv = defocus - c.dfdiff;
+    d.dfdiff = c.dfdiff;
+    d.dfang = c.dfang;
+    d.lambda = (float)(12.2639 / sqrt((double)p.energy * 1000.0 + 0.97845 * (double)p.energy * (double)p.energy));
+    d.cs = p.cs;
+    d.ampconst = p.ampconst;
+    if (ds_out) *ds_out = 1.0f / (p.apix * (float)padding_for_ds);
+    return d;
+}
+
+int adjust_padding(int window, int tx, int ty) {
+    // main.cu:158-178
+    if (window < tx || window < ty) {
+        int l = 0;
+        while (l < tx || l < ty) l += 32;
+        return l;
+    }
+    return window;
+}
+
+unsigned blocks_for(long long n, int threads, unsigned cap = 1u << 30) {
+    long long b = (n + threads - 1) / threads;
+    if (b < 1) b = 1;
+    return (unsigned)std::min<long long>(b, cap);
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* gs_status_string(int s) {
+    switch (s) {
+        case GS_OK: return "ok";
+        case GS_ERR_ARG: return "invalid argument";
+        case GS_ERR_OOM: return "out of memory";
+        case GS_ERR_CUDA: return "CUDA error";
+        case GS_ERR_STATE: return "invalid call order";
+        case GS_ERR_UNSUPPORTED: return "unsupported input";
+        case GS_ERR_TIMEOUT: return "device wait timed out";
+        case GS_ERR_IO: return "I/O error";
+        default: return "unknown status";
+    }
+}
+
+int gs_version(void) { return 10000; }
+
+int gs_params_default(gs_params* p) {
+    if (!p) return GS_ERR_ARG;
+    // DataReader.h:16-42
+    p->apix = -1; p->phi_step = -1; p->kk = -1; p->energy = -1; p->cs = -1;
+    p->highres = -1; p->lowres = -1; p->d_m = -1;
+    p->thres = 7.0f;
+    p->window_size = 320;
+    p->overlap = -1;
+    p->phase_flip = 0;
+    p->norm_type = 0;
+    p->invert = 0;
+    p->ampconst = 0.07f;
+    p->a = -9.32f; p->b = 2.65f; p->b2 = 0.01908f;
+    p->bfactor = -78.7757f; p->bfactor2 = -12.9121f; p->bfactor3 = 1.28732f;
+    p->precision = GS_PREC_FP32;
+    return GS_OK;
+}
+
+int gs_ctx_create(int device, gs_ctx** out) {
+    if (!out) return GS_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return GS_ERR_CUDA;
+    }
+    if (device < 0 || device >= ndev) return GS_ERR_ARG;
+    gs_ctx* ctx = new gs_ctx();
+    ctx->device = device;
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        delete ctx;
+        return GS_ERR_CUDA;
+    }
+    *out = ctx;
+    return GS_OK;
+}
+
+int gs_ctx_destroy(gs_ctx* ctx) {
+    if (!ctx) return GS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (auto& kv : ctx->plans) cudaFree(kv.second.tw);
+    DBuf* bufs[] = {&ctx->tmpl, &ctx->in, &ctx->q, &ctx->cimg, &ctx->img, &ctx->stats, &ctx->ra, &ctx->rb,
+                    &ctx->off, &ctx->win, &ctx->wsum, &ctx->winv, &ctx->tspec, &ctx->scratch, &ctx->pstats,
+                    &ctx->coef, &ctx->acc, &ctx->units, &ctx->picks, &ctx->count};
+    for (DBuf* b : bufs) free_buf(*b);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return GS_OK;
+}
+
+const char* gs_ctx_last_error(gs_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+static int validate_params(gs_ctx* ctx, const gs_params* p) {
+    if (!(p->apix > 0) || !(p->phi_step > 0) || !(p->kk >= 0) || !(p->energy > 0) || !(p->cs >= 0) ||
+        !(p->highres > 0) || !(p->lowres > 0) || !(p->d_m > 0))
+        return set_err(ctx, GS_ERR_ARG, "required parameter missing or not positive");
+    if (p->norm_type != 0) return set_err(ctx, GS_ERR_UNSUPPORTED, "norm_type %d is not implemented", p->norm_type);
+    if (p->precision != GS_PREC_FP32) return set_err(ctx, GS_ERR_UNSUPPORTED, "precision mode %d", p->precision);
+    if (p->window_size <= 0) return set_err(ctx, GS_ERR_ARG, "window_size must be positive");
+    if (360.0f / p->phi_step > 1e6f) return set_err(ctx, GS_ERR_ARG, "phistep too small");
+    return GS_OK;
+}
+
+int gs_set_templates(gs_ctx* ctx, const gs_params* p, const float* host_templates, int n, int tx, int ty,
+                     const gs_ctf* first_ctf) {
+    if (!ctx || !p || !host_templates || !first_ctf || n <= 0 || tx <= 0 || ty <= 0)
+        return set_err(ctx, GS_ERR_ARG, "null pointer or empty template stack");
+    TRY(validate_params(ctx, p));
+    if (n > 2 * 65535) return set_err(ctx, GS_ERR_UNSUPPORTED, "at most %d templates", 2 * 65535);
+    CK(cudaSetDevice(ctx->device));
+    const int l = adjust_padding(p->window_size, tx, ty);
+    if (l % 2) return set_err(ctx, GS_ERR_UNSUPPORTED, "window size %d must be even", l);
+    ctx->have_tmpl = false;
+    ctx->have_units = false;
+    ctx->p = *p;
+    ctx->ctf0 = *first_ctf;
+    ctx->l = l;
+    ctx->ntmpl = n;
+    ctx->tx = tx;
+    ctx->ty = ty;
+    const size_t l2 = (size_t)l * l;
+    TRY(ensure(ctx, ctx->tmpl, sizeof(float) * l2 * n));
+    const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)n, (size_t)(1u << 30) / (l2 * 8)));
+    DBuf raw, F, div, sumsq, inv, wmap;
+    int st = GS_OK;
+    do {
+        if ((st = ensure(ctx, raw, sizeof(float) * (size_t)tx * ty * chunk))) break;
+        if ((st = ensure(ctx, F, sizeof(float2) * l2 * chunk))) break;
+        if ((st = ensure(ctx, div, sizeof(float) * (size_t)(l / 2) * chunk))) break;
+        if ((st = ensure(ctx, sumsq, sizeof(double) * 2 * chunk))) break;
+        if ((st = ensure(ctx, inv, sizeof(double) * chunk))) break;
+        if ((st = ensure(ctx, wmap, sizeof(float) * l2))) break;
+        // weight map with the FIRST micrograph's CTF; ds from the configured
+        // window size (main.cu:155 runs before main.cu:1116 adjusts it)
+        float ds = 0.0f;
+        CtfDev c0 = make_ctf(*p, *first_ctf, p->window_size, &ds);
+        WeightConsts wc;
+        wc.hp = ((float)l * p->apix) / p->highres;
+        wc.lp = ((float)l * p->apix) / p->lowres;
+        wc.ds = ds;
+        wc.kk = p->kk; wc.a = p->a; wc.b = p->b; wc.b2 = p->b2;
+        wc.bf = p->bfactor; wc.bf2 = p->bfactor2; wc.bf3 = p->bfactor3;
+        k_weight_map<<<blocks_for((long long)l2, 256), 256, 0, ctx->stream>>>(P<float>(wmap), l, wc, c0);
+        if ((st = (cudaGetLastError() == cudaSuccess ? GS_OK : set_err(ctx, GS_ERR_CUDA, "k_weight_map")))) break;
+        for (int c0i = 0; c0i < n && st == GS_OK; c0i += chunk) {
+            const int nc = std::min(chunk, n - c0i);
+            cudaError_t e = cudaMemcpyAsync(P<float>(raw), host_templates + (size_t)c0i * tx * ty,
+                                            sizeof(float) * (size_t)tx * ty * nc, cudaMemcpyHostToDevice, ctx->stream);
+            if (e != cudaSuccess) { st = set_err(ctx, GS_ERR_CUDA, "template upload: %s", cudaGetErrorString(e)); break; }
+            k_tmpl_pad_edge<<<nc, 256, 0, ctx->stream>>>(P<float>(raw), tx, ty, l, P<float2>(F));
+            if (cudaGetLastError() != cudaSuccess) { st = set_err(ctx, GS_ERR_CUDA, "k_tmpl_pad_edge"); break; }
+            if ((st = run_fft<false>(ctx, l, rows_of(l, l), nc, IoComplex{P<float2>(F), 1.0f}))) break;
+            if ((st = run_fft<false>(ctx, l, cols_of(l, l), nc, IoComplex{P<float2>(F), 1.0f / (float)l2}))) break;
+            const size_t shs = (size_t)(l / 2) * (sizeof(double) + sizeof(unsigned));
+            if (shs > kMaxSmem) { st = set_err(ctx, GS_ERR_UNSUPPORTED, "window too large"); break; }
+            cudaFuncSetAttribute(k_tmpl_shells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shs);
+            k_tmpl_shells<<<nc, 256, shs, ctx->stream>>>(P<float2>(F), l, P<float>(div));
+            cudaMemsetAsync(P<double>(sumsq), 0, sizeof(double) * 2 * nc, ctx->stream);
+            dim3 g(blocks_for((long long)l2, 256, 64), nc);
+            k_tmpl_apply<<<g, 256, 0, ctx->stream>>>(P<float2>(F), l, P<float>(div), P<float>(wmap), P<double>(sumsq));
+            k_inv_amp_norm<<<blocks_for(nc, 128), 128, 0, ctx->stream>>>(P<double>(sumsq), nc, P<double>(inv));
+            if (cudaGetLastError() != cudaSuccess) { st = set_err(ctx, GS_ERR_CUDA, "template weighting"); break; }
+            if ((st = run_fft<true>(ctx, l, rows_of(l, l), nc, IoScaleIn{P<float2>(F), P<double>(inv)}))) break;
+            if ((st = run_fft<true>(ctx, l, cols_of(l, l), nc,
+                                    IoRealOut{P<float2>(F), P<float>(ctx->tmpl) + (size_t)c0i * l2, 1.0f}))) break;
+        }
+        if (st) break;
+        cudaError_t e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) st = set_err(ctx, GS_ERR_CUDA, "template preprocessing: %s", cudaGetErrorString(e));
+    } while (0);
+    cudaStreamSynchronize(ctx->stream);
+    free_buf(raw); free_buf(F); free_buf(div); free_buf(sumsq); free_buf(inv); free_buf(wmap);
+    if (st == GS_OK) ctx->have_tmpl = true;
+    return st;
+}
+
+int gs_get_geometry(gs_ctx* ctx, int nx, int ny, gs_geometry* out) {
+    if (!ctx || !out || nx <= 0 || ny <= 0) return set_err(ctx, GS_ERR_ARG, "bad geometry query");
+    if (!ctx->have_tmpl) return set_err(ctx, GS_ERR_STATE, "templates not loaded");
+    const int l = ctx->l;
+    if (l - ctx->p.overlap <= 0) return set_err(ctx, GS_ERR_ARG, "overlap must be smaller than the window");
+    out->l = l;
+    out->n_windows_x = (int)window_offsets(nx, l, ctx->p.overlap).size();
+    out->n_windows_y = (int)window_offsets(ny, l, ctx->p.overlap).size();
+    out->n_angles = (int)angle_list(ctx->p.phi_step).size();
+    out->n_templates = ctx->ntmpl;
+    return GS_OK;
+}
+
+static int search_impl(gs_ctx* ctx, const float* d_mic, int nx, int ny, const gs_ctf* ctf, gs_pick** picks,
+                       size_t* n_picks) {
+    const gs_params& p = ctx->p;
+    const int l = ctx->l;
+    const long long l2 = (long long)l * l;
+    const int N = ctx->ntmpl;
+    const int Np = (N + 1) / 2;
+    const long long npix = (long long)nx * ny;
+    if (l - p.overlap <= 0) return set_err(ctx, GS_ERR_ARG, "overlap must be smaller than the window");
+    if (std::max(nx, ny) / 2 > 1 << 20) return set_err(ctx, GS_ERR_UNSUPPORTED, "micrograph too large");
+    const std::vector<int> offx = window_offsets(nx, l, p.overlap), offy = window_offsets(ny, l, p.overlap);
+    const int bx = (int)offx.size(), by = (int)offy.size(), nw = bx * by;
+    const std::vector<float> angles = angle_list(p.phi_step);
+    const int na = (int)angles.size();
+    const long long total_units = (long long)na * nw * N;
+
+    cudaEvent_t ev[4];
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    struct EvGuard { cudaEvent_t* e; ~EvGuard() { for (int i = 0; i < 4; ++i) cudaEventDestroy(e[i]); } } evg{ev};
+    CK(cudaEventRecord(ev[0], ctx->stream));
+
+    // ---- micrograph: init_d_image (main.cu:523-586) ----
+    TRY(ensure(ctx, ctx->q, sizeof(float) * 2 * npix));
+    TRY(ensure(ctx, ctx->cimg, sizeof(float2) * npix));
+    TRY(ensure(ctx, ctx->img, sizeof(float) * npix));
+    TRY(ensure(ctx, ctx->stats, sizeof(MicStats)));
+    const int ns = std::max(nx, ny) / 2;
+    TRY(ensure(ctx, ctx->ra, sizeof(double) * ns));
+    TRY(ensure(ctx, ctx->rb, sizeof(unsigned) * ns));
+    float* q1 = P<float>(ctx->q);
+    float* q2 = q1 + npix;
+    k_mic_quot<<<blocks_for(npix, 256), 256, 0, ctx->stream>>>(d_mic, npix, nx, ny, q1, q2);
+    k_mic_seq<<<1, 32, 0, ctx->stream>>>(q1, q2, npix, P<MicStats>(ctx->stats));
+    k_mic_clamp<<<blocks_for(npix, 256), 256, 0, ctx->stream>>>(d_mic, npix, P<MicStats>(ctx->stats), p.invert,
+                                                                 P<float2>(ctx->cimg));
+    CKL();
+    float2* C = P<float2>(ctx->cimg);
+    TRY(run_fft<false>(ctx, nx, rows_of(nx, ny), 1, IoComplex{C, 1.0f}));
+    TRY(run_fft<false>(ctx, ny, cols_of(nx, ny), 1, IoComplex{C, (float)(1.0 / (double)npix)}));
+    CtfDev cm = make_ctf(p, *ctf, l, nullptr);
+    if (p.phase_flip == 1) {
+        CK(cudaMemsetAsync(ctx->ra.p, 0, sizeof(double) * ns, ctx->stream));
+        CK(cudaMemsetAsync(ctx->rb.p, 0, sizeof(unsigned) * ns, ctx->stream));
+        const size_t shs = (size_t)ns * (sizeof(double) + sizeof(unsigned));
+        if (shs > kMaxSmem) return set_err(ctx, GS_ERR_UNSUPPORTED, "micrograph too large for the shell histogram");
+        CK(cudaFuncSetAttribute(k_mic_flip_shells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shs));
+        const unsigned nb = (unsigned)std::min(ny, 296);
+        k_mic_flip_shells<<<nb, 256, shs, ctx->stream>>>(C, nx, ny, cm, P<double>(ctx->ra), P<unsigned>(ctx->rb));
+        MicWhitenConsts w;
+        const int L = std::max(nx, ny);
+        w.apix = p.apix;
+        w.hp = ((float)L * p.apix) / p.highres;
+        w.lp = ((float)L * p.apix) / p.lowres;
+        w.damp = ((float)L * p.apix) / 6.0f;
+        w.kk = p.kk; w.a = p.a; w.b = p.b; w.b2 = p.b2;
+        w.bf = p.bfactor; w.bf2 = p.bfactor2; w.bf3 = p.bfactor3;
+        k_mic_whiten<<<blocks_for(npix, 256), 256, 0, ctx->stream>>>(C, nx, ny, cm, w, P<double>(ctx->ra),
+                                                                      P<unsigned>(ctx->rb));
+    } else {
+        k_set_dc_zero<<<1, 1, 0, ctx->stream>>>(C);
+    }
+    CKL();
+    TRY(run_fft<true>(ctx, ny, cols_of(nx, ny), 1, IoComplex{C, 1.0f}));
+    TRY(run_fft<true>(ctx, nx, rows_of(nx, ny), 1, IoRealOut{C, P<float>(ctx->img), 1.0f}));
+
+    // ---- windows: split_normalize_image + fft_on_img (main.cu:588-655, 758-769) ----
+    TRY(ensure(ctx, ctx->off, sizeof(int) * (bx + by)));
+    std::vector<int> offs(offx);
+    offs.insert(offs.end(), offy.begin(), offy.end());
+    CK(cudaMemcpyAsync(ctx->off.p, offs.data(), sizeof(int) * offs.size(), cudaMemcpyHostToDevice, ctx->stream));
+    const int* d_offx = P<int>(ctx->off);
+    const int* d_offy = d_offx + bx;
+    TRY(ensure(ctx, ctx->win, sizeof(float2) * l2 * nw));
+    float2* W = P<float2>(ctx->win);
+    {
+        dim3 g(blocks_for(l2, 256, 256), nw);
+        k_extract_windows<<<g, 256, 0, ctx->stream>>>(P<float>(ctx->img), nx, ny, d_offx, d_offy, bx, l, W);
+        CKL();
+    }
+    TRY(run_fft<false>(ctx, l, rows_of(l, l), nw, IoComplex{W, 1.0f}));
+    TRY(run_fft<false>(ctx, l, cols_of(l, l), nw, IoComplex{W, (float)(1.0 / (double)l2)}));
+    if (p.phase_flip == 1) {
+        TRY(ensure(ctx, ctx->wsum, sizeof(double) * 2 * nw));
+        TRY(ensure(ctx, ctx->winv, sizeof(double) * nw));
+        CK(cudaMemsetAsync(ctx->wsum.p, 0, sizeof(double) * 2 * nw, ctx->stream));
+        dim3 g(blocks_for(l2 / 2, 256, 64), nw);
+        k_win_sumsq<<<g, 256, 0, ctx->stream>>>(W, l, P<double>(ctx->wsum));
+        k_inv_amp_norm<<<blocks_for(nw, 128), 128, 0, ctx->stream>>>(P<double>(ctx->wsum), nw, P<double>(ctx->winv));
+        dim3 g2(blocks_for(l2, 256, 256), nw);
+        k_scale_images<<<g2, 256, 0, ctx->stream>>>(W, l2, P<double>(ctx->winv));
+        CKL();
+    }
+    CK(cudaEventRecord(ev[1], ctx->stream));
+
+    // ---- angle loop (main.cu:1232-1257) ----
+    TRY(ensure(ctx, ctx->tspec, sizeof(float2) * l2 * Np));
+    TRY(ensure(ctx, ctx->scratch, sizeof(float2) * l2 * Np));
+    TRY(ensure(ctx, ctx->pstats, sizeof(double) * 2 * N));
+    TRY(ensure(ctx, ctx->coef, sizeof(float4) * Np));
+    TRY(ensure(ctx, ctx->acc, sizeof(UnitAcc) * N));
+    TRY(ensure(ctx, ctx->units, sizeof(UnitOut) * std::max<long long>(1, total_units)));
+    float2* TS = P<float2>(ctx->tspec);
+    float2* R = P<float2>(ctx->scratch);
+    UnitAcc* acc = P<UnitAcc>(ctx->acc);
+    UnitOut* units = P<UnitOut>(ctx->units);
+    const float q_lo = p.d_m / 4.0f;
+    const float q_hi = (float)l - q_lo;
+    const float sgn = ((l / 2) % 2 == 0) ? 1.0f : -1.0f;
+    float ms_spec = 0.0f, ms_corr = 0.0f;
+    cudaEvent_t ea, eb, ec;
+    CK(cudaEventCreate(&ea));
+    CK(cudaEventCreate(&eb));
+    CK(cudaEventCreate(&ec));
+    struct EvGuard3 { cudaEvent_t a, b, c; ~EvGuard3() { cudaEventDestroy(a); cudaEventDestroy(b); cudaEventDestroy(c); } } eg3{ea, eb, ec};
+    for (int ai = 0; ai < na; ++ai) {
+        const float e = angles[ai];
+        const double ang = (double)e * kPiRef / 180.0;
+        const float cose = (float)cos(ang), sine = (float)sin(ang);
+        CK(cudaEventRecord(ea, ctx->stream));
+        CK(cudaMemsetAsync(ctx->pstats.p, 0, sizeof(double) * 2 * N, ctx->stream));
+        {
+            dim3 g(blocks_for(l2, 256, 32), Np);
+            k_pair_rotate<<<g, 256, 0, ctx->stream>>>(P<float>(ctx->tmpl), N, l, cose, sine, p.d_m, TS,
+                                                      P<double>(ctx->pstats));
+            k_pair_coef<<<blocks_for(Np, 128), 128, 0, ctx->stream>>>(P<double>(ctx->pstats), N, l,
+                                                                       P<float4>(ctx->coef));
+            CKL();
+        }
+        TRY(run_fft<false>(ctx, l, rows_of(l, l), Np, IoPairNorm{TS, P<float4>(ctx->coef), l2}));
+        TRY(run_fft<false>(ctx, l, cols_of(l, l), Np, IoComplex{TS, (float)(1.0 / (double)l2)}));
+        CK(cudaEventRecord(eb, ctx->stream));
+        for (int w = 0; w < nw; ++w) {
+            CK(cudaMemsetAsync(acc, 0, sizeof(UnitAcc) * N, ctx->stream));
+            TRY(run_fft<true>(ctx, l, rows_of(l, l), Np, IoPass1{W + (size_t)w * l2, TS, R, l2}));
+            IoPass2 io2;
+            io2.R = R; io2.acc = acc; io2.l = l; io2.ntmpl = N; io2.q_lo = q_lo; io2.q_hi = q_hi; io2.sgn = sgn;
+            TRY(run_fft<true>(ctx, l, cols_of(l, l), Np, io2));
+            k_finalize<<<blocks_for(N, 128), 128, 0, ctx->stream>>>(acc, N, l,
+                                                                    units + ((size_t)ai * nw + w) * N);
+            CKL();
+        }
+        CK(cudaEventRecord(ec, ctx->stream));
+        CK(cudaEventSynchronize(ec));
+        float t1 = 0, t2 = 0;
+        cudaEventElapsedTime(&t1, ea, eb);
+        cudaEventElapsedTime(&t2, eb, ec);
+        ms_spec += t1;
+        ms_corr += t2;
+    }
+    ctx->last_na = na;
+    ctx->last_nw = nw;
+    ctx->last_nt = N;
+    ctx->have_units = true;
+
+    // ---- picks (main.cu:869-891), reference order restored by sorting ----
+    TRY(ensure(ctx, ctx->picks, sizeof(PickDev) * std::max<long long>(1, total_units)));
+    TRY(ensure(ctx, ctx->count, sizeof(unsigned long long)));
+    CK(cudaMemsetAsync(ctx->count.p, 0, sizeof(unsigned long long), ctx->stream));
+    if (total_units > 0) {
+        k_compact<<<blocks_for(total_units, 256), 256, 0, ctx->stream>>>(
+            units, total_units, nw, N, bx, d_offx, d_offy, l, p.d_m, nx, ny, p.thres, P<PickDev>(ctx->picks),
+            P<unsigned long long>(ctx->count), total_units);
+        CKL();
+    }
+    unsigned long long cnt = 0;
+    CK(cudaMemcpyAsync(&cnt, ctx->count.p, sizeof cnt, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    std::vector<PickDev> hp(cnt);
+    if (cnt) CK(cudaMemcpy(hp.data(), ctx->picks.p, sizeof(PickDev) * cnt, cudaMemcpyDeviceToHost));
+    CK(cudaEventRecord(ev[3], ctx->stream));
+    CK(cudaEventSynchronize(ev[3]));
+    std::sort(hp.begin(), hp.end(), [](const PickDev& a, const PickDev& b) { return a.unit < b.unit; });
+    gs_pick* out = nullptr;
+    if (cnt) {
+        out = (gs_pick*)malloc(sizeof(gs_pick) * cnt);
+        if (!out) return set_err(ctx, GS_ERR_OOM, "host allocation of %llu picks", cnt);
+        for (size_t k = 0; k < cnt; ++k) {
+            const long long u = hp[k].unit;
+            const int J = (int)(u % N);
+            const int w = (int)((u / N) % nw);
+            const int ai = (int)(u / ((long long)N * nw));
+            gs_pick& o = out[k];
+            o.angle_index = ai;
+            o.phi = printed_phi(angles[ai]);
+            o.window_x = w % bx;
+            o.window_y = w / bx;
+            o.template_index = J;
+            o.center_x = hp[k].cx;
+            o.center_y = hp[k].cy;
+            o.score = hp[k].score;
+        }
+    }
+    *picks = out;
+    *n_picks = (size_t)cnt;
+    float t_prep = 0, t_tot = 0;
+    cudaEventElapsedTime(&t_prep, ev[0], ev[1]);
+    cudaEventElapsedTime(&t_tot, ev[0], ev[3]);
+    ctx->timings[0] = t_prep;
+    ctx->timings[1] = ms_spec;
+    ctx->timings[2] = ms_corr;
+    ctx->timings[3] = t_tot;
+    return GS_OK;
+}
+
+int gs_search_device(gs_ctx* ctx, const float* device_micrograph, int nx, int ny, const gs_ctf* ctf, gs_pick** picks,
+                     size_t* n_picks) {
+    if (!ctx || !device_micrograph || !ctf || !picks || !n_picks || nx <= 0 || ny <= 0)
+        return set_err(ctx, GS_ERR_ARG, "null pointer or empty micrograph");
+    *picks = nullptr;
+    *n_picks = 0;
+    if (!ctx->have_tmpl) return set_err(ctx, GS_ERR_STATE, "gs_set_templates must come first");
+    CK(cudaSetDevice(ctx->device));
+    return search_impl(ctx, device_micrograph, nx, ny, ctf, picks, n_picks);
+}
+
+int gs_search(gs_ctx* ctx, const float* host_micrograph, int nx, int ny, const gs_ctf* ctf, gs_pick** picks,
+              size_t* n_picks) {
+    if (!ctx || !host_micrograph || !ctf || !picks || !n_picks || nx <= 0 || ny <= 0)
+        return set_err(ctx, GS_ERR_ARG, "null pointer or empty micrograph");
+    *picks = nullptr;
+    *n_picks = 0;
+    if (!ctx->have_tmpl) return set_err(ctx, GS_ERR_STATE, "gs_set_templates must come first");
+    CK(cudaSetDevice(ctx->device));
+    const size_t bytes = sizeof(float) * (size_t)nx * ny;
+    TRY(ensure(ctx, ctx->in, bytes));
+    CK(cudaMemcpyAsync(ctx->in.p, host_micrograph, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    return search_impl(ctx, P<float>(ctx->in), nx, ny, ctf, picks, n_picks);
+}
+
+int gs_get_units(gs_ctx* ctx, gs_unit* host_out, size_t cap, size_t* n_out) {
+    if (!ctx || !n_out) return set_err(ctx, GS_ERR_ARG, "null pointer");
+    if (!ctx->have_units) return set_err(ctx, GS_ERR_STATE, "no search has run");
+    const size_t total = (size_t)ctx->last_na * ctx->last_nw * ctx->last_nt;
+    *n_out = total;
+    if (!host_out) return GS_OK;
+    if (cap < total) return set_err(ctx, GS_ERR_ARG, "capacity %zu < %zu units", cap, total);
+    static_assert(sizeof(gs_unit) == sizeof(UnitOut), "gs_unit layout");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpy(host_out, ctx->units.p, sizeof(gs_unit) * total, cudaMemcpyDeviceToHost));
+    return GS_OK;
+}
+
+void gs_picks_free(gs_pick* p) { free(p); }
+
+int gs_get_timings(gs_ctx* ctx, float* ms4) {
+    if (!ctx || !ms4) return GS_ERR_ARG;
+    for (int i = 0; i < 4; ++i) ms4[i] = ctx->timings[i];
+    return GS_OK;
+}
+
+}  // extern "C"

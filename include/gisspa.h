@@ -1,0 +1,159 @@
+/*
+ * gisspa.h -- C ABI of the B200-native GisSPA template-matching search.
+ *
+ * The reference (Autumn1998/GisSPA) has no library interface: its boundary is
+ * the `./main <config>` process, and its search lives in host functions that
+ * take raw cufftComplex device buffers (main.cu).  Each entry point below
+ * replaces one of those host stages; the comment names the reference code it
+ * stands in for.  The drop-in CLI (gisspa_main, csrc/driver) and the Python
+ * wrapper (gisspa_b200/__init__.py) call only these functions.
+ *
+ * Conventions
+ *  - Every function returns an int status (GS_OK == 0).  Nothing calls exit().
+ *  - Pointers named host_* are host memory owned by the caller; the context
+ *    owns all device memory it allocates.  *_device entry points take device
+ *    pointers on the context's device.
+ *  - One context per host thread; a context runs its work on its own CUDA
+ *    stream and calls on one context must not overlap.
+ *  - Angles are degrees, defocus values micrometres exactly as written in the
+ *    reference's input list (positive = underfocus).
+ */
+#ifndef GISSPA_H
+#define GISSPA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference prints and exit(-1)s on every failure
+ * (GPU_func.cuh:33-41); here each failure is returned to the caller. */
+#define GS_OK 0
+#define GS_ERR_ARG 1         /* bad argument (null pointer, size, geometry) */
+#define GS_ERR_OOM 2         /* device or host allocation failed */
+#define GS_ERR_CUDA 3        /* a CUDA runtime call or kernel failed */
+#define GS_ERR_STATE 4       /* call out of order (e.g. search before templates) */
+#define GS_ERR_UNSUPPORTED 5 /* valid input outside what this build handles */
+#define GS_ERR_TIMEOUT 6     /* a bounded device wait gave up */
+#define GS_ERR_IO 7          /* file could not be read or written */
+
+/* Search parameters: the numeric fields of the reference's
+ * struct Parameters (EMReader/DataReader.h:14-42), same meaning and defaults
+ * (see gs_params_default). */
+typedef struct gs_params {
+    float apix;        /* angpix: pixel size, A */
+    float phi_step;    /* phistep: in-plane angle step, deg */
+    float kk;          /* kk: overlapping density parameter */
+    float energy;      /* energy: kV */
+    float cs;          /* cs: spherical aberration, mm */
+    float highres;     /* Highres: high-resolution cut, A */
+    float lowres;      /* Lowres: low-resolution cut, A */
+    float d_m;         /* diameter: particle diameter, px */
+    float thres;       /* threshold: score threshold (default 7) */
+    int window_size;   /* window_size: window l (default 320) */
+    int overlap;       /* overlap between windows, px (default -1) */
+    int phase_flip;    /* phase_flip 0/1 (default 0) */
+    int norm_type;     /* norm_type: only 0 is implemented (default 0) */
+    int invert;        /* invert 0/1 (default 0) */
+    float ampconst;    /* amplitude contrast (fixed 0.07 in the reference) */
+    float a, b, b2;    /* noise-curve constants (DataReader.h:25) */
+    float bfactor, bfactor2, bfactor3; /* signal-curve constants */
+    int precision;     /* GS_PREC_FP32 (the only mode in this build) */
+} gs_params;
+
+#define GS_PREC_FP32 0
+
+/* Per-micrograph CTF line values as in the input list
+ * (DataReader.cpp:366-388: defocus=, dfdiff=, dfang=). */
+typedef struct gs_ctf {
+    float defocus; /* um, positive underfocus */
+    float dfdiff;  /* um */
+    float dfang;   /* deg */
+} gs_ctf;
+
+/* One output line of the reference's writeScoreToDisk (main.cu:974-989). */
+typedef struct gs_pick {
+    int angle_index;   /* index in the in-plane angle loop */
+    float phi;         /* third Euler angle as printed: 360 - euler3, wrapped */
+    int window_x;      /* window column i */
+    int window_y;      /* window row j */
+    int template_index;/* J (row of the Euler file) */
+    float center_x;    /* micrograph pixel x of the peak */
+    float center_y;
+    float score;       /* peak / sigma-without-peak */
+} gs_pick;
+
+/* Per (angle, window, template) result of the last search, dense. */
+typedef struct gs_unit {
+    float score;  /* NaN when the map had zero variance (no pick possible) */
+    int pos;      /* argmax flat index y*l + x in window coordinates */
+    float peak;   /* max(0, border-masked max) */
+    float sigma;  /* std of the map without the peak */
+} gs_unit;
+
+/* Search geometry derived from the parameters, templates and micrograph. */
+typedef struct gs_geometry {
+    int l;          /* window size after the template-size adjustment */
+    int n_windows_x;
+    int n_windows_y;
+    int n_angles;
+    int n_templates;
+} gs_geometry;
+
+const char* gs_status_string(int status);
+int gs_version(void);
+
+/* Reference defaults of struct Parameters (DataReader.h:16-42); required
+ * keys are set to -1 like the reference's "not given" marker. */
+int gs_params_default(gs_params* p);
+
+/* Context on one CUDA device; replaces main.cu:1071 cudaSetDevice + the
+ * stream of main.cu:274.  Owns a stream and all device buffers. */
+int gs_ctx_create(int device, struct gs_ctx** out);
+int gs_ctx_destroy(struct gs_ctx* ctx);
+/* Last error text of this context ("" if none). */
+const char* gs_ctx_last_error(struct gs_ctx* ctx);
+
+/* Template preprocessing, once per run.  Replaces readAndPaddingTemplate +
+ * edgeNormalize + handleTemplate (main.cu:182-474): pad to l x l, edge-ring
+ * normalise, whiten by radial shells, band-pass and |CTF| x Wiener weight with
+ * `first_ctf` (the reference weights every template with the FIRST
+ * micrograph's CTF, main.cu:1106), amplitude-normalise, inverse FFT.
+ * host_templates: n x ty x tx float32, row-major. */
+int gs_set_templates(struct gs_ctx* ctx, const gs_params* p, const float* host_templates,
+                     int n, int tx, int ty, const gs_ctf* first_ctf);
+
+/* Geometry of a search of an nx x ny micrograph with the loaded templates. */
+int gs_get_geometry(struct gs_ctx* ctx, int nx, int ny, gs_geometry* out);
+
+/* One micrograph, norm_type 0.  Replaces init_d_image +
+ * split_normalize_image + fft_on_img + the angle loop of rotateTemplate and
+ * pickPartcles_IMG_NORM (main.cu:523-894, 1230-1257).  Picks come back in
+ * the reference's line order (angle, window row, window column, template);
+ * *picks is allocated by the library, release it with gs_picks_free.
+ * host_micrograph: ny x nx float32 row-major. */
+int gs_search(struct gs_ctx* ctx, const float* host_micrograph, int nx, int ny,
+              const gs_ctf* ctf, gs_pick** picks, size_t* n_picks);
+
+/* Same search with the micrograph already in device memory (ny x nx float32
+ * on the context's device).  The micrograph is not modified. */
+int gs_search_device(struct gs_ctx* ctx, const float* device_micrograph, int nx, int ny,
+                     const gs_ctf* ctf, gs_pick** picks, size_t* n_picks);
+
+/* Copy the dense per-unit table of the last search (n_angles x n_windows x
+ * n_templates, that order) into host memory; cap is the element capacity. */
+int gs_get_units(struct gs_ctx* ctx, gs_unit* host_out, size_t cap, size_t* n_out);
+
+void gs_picks_free(gs_pick* picks);
+
+/* Timings of the last search, milliseconds, measured with CUDA events on the
+ * context's stream: [0] micrograph preprocessing, [1] template spectra (all
+ * angles), [2] correlation passes (all angles), [3] total. */
+int gs_get_timings(struct gs_ctx* ctx, float* ms4);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GISSPA_H */
