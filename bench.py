@@ -1,0 +1,438 @@
+#!/usr/bin/env python
+"""Throughput of the GisSPA 2D template-matching search, in micrographs/s.
+
+Default workload (N=1): one 5760 x 4092 float32 micrograph with 400 pasted
+particles at SNR 0.03 and 1/f^0.5 coloured noise, 2000 templates of
+200 x 200, 72 in-plane angles (5 deg), window 720 with overlap 200, defocus
+0.8-2.5 um with up to 500 A astigmatism.  Inputs are seeded synthetic data
+(gisspa_b200.synth).  A step = one whole micrograph through the search
+(preprocessing, window spectra, 72 angles x 88 windows x 2000 templates of
+correlation, picks).  Template preprocessing runs once per run, before
+timing, and is reported as template_prep_s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload full|small]
+
+N > 1 runs under torch.distributed.run: every rank searches its own
+micrograph (replicas; no collective on the data path), the timed region is
+bracketed by barriers, and the time is the max over ranks.
+
+--impl reference times the reference GisSPA binary (oracle/_ref, the
+reference's own sources built for sm_100a) on the same micrograph and
+templates.  Its kernels need window % 32 == 0, so it runs at window 768
+(the nearest legal size) on a bounded sample of in-plane angles and the
+per-micrograph time is extrapolated linearly in angles.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "micrographs/s"
+UNIT = "micrographs/s"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+def workload_kwargs(name: str, window: int = None):
+    from gisspa_b200 import synth
+    if name == "full":
+        kw = synth.config_full(seed=1)
+    elif name == "small":
+        kw = synth.config_small(seed=0)
+    else:
+        raise ValueError(name)
+    if window is not None:
+        kw["window"] = window
+    return kw
+
+
+def make_data(name: str, seed_offset: int = 0, window: int = None):
+    from gisspa_b200 import synth
+    kw = workload_kwargs(name, window)
+    seed = kw.pop("seed") + seed_offset
+    return synth.make_dataset(seed, **kw), kw
+
+
+def params_for(ds, kw):
+    import gisspa_b200 as G
+    p = ds.params
+    return G.default_params(apix=float(p["angpix"]), phi_step=float(p["phistep"]), kk=float(p["kk"]),
+                            energy=float(p["energy"]), cs=float(p["cs"]), highres=float(p["Highres"]),
+                            lowres=float(p["Lowres"]), d_m=float(p["diameter"]),
+                            thres=float(p["threshold"]), window_size=int(p["window_size"]),
+                            overlap=int(p["overlap"]), phase_flip=int(p["phase_flip"]),
+                            invert=int(p["invert"]))
+
+
+def unit_flops(l: int) -> float:
+    """Algorithmic FLOPs of one (template, angle, window) unit: a real-input
+    l x l inverse FFT (2.5 n log2 n) plus the conjugate product and the
+    max / sum / sum-of-squares epilogue (3 l^2 each)."""
+    n = l * l
+    return 2.5 * n * math.log2(n) + 6.0 * n
+
+
+def micrograph_flops(l, nt, na, nw, nx, ny) -> float:
+    """F = Nt Na (2.5 l^2 log2 l^2 + 14 l^2) + Nt Na Nw (unit) + 5 nx ny log2(nx ny)
+    + 3 Nw 2.5 l^2 log2 l^2 (template spectra, units, micrograph and window FFTs)."""
+    n = l * l
+    return (nt * na * (2.5 * n * math.log2(n) + 14 * n) + nt * na * nw * unit_flops(l)
+            + 5.0 * nx * ny * math.log2(nx * ny) + 3 * nw * 2.5 * n * math.log2(n))
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi sampling of SM clock and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        if shutil.which("nvidia-smi") is None:
+            return
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                      "--format=csv,noheader,nounits", "-lms", "200"],
+                                     stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        sm = [r[0] for r in rows]
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return json.load(fh), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle (FP32 FFTs, all host threads) on a bounded sample
+# ---------------------------------------------------------------------------
+def cpu_baseline(ds, kw, geom) -> dict:
+    from oracle import gisspa_oracle as O
+    cores = os.cpu_count() or 1
+    m = ds.micrographs[0]
+    p = O.Params(apix=kw.get("apix", 1.0), phi_step=kw["phistep"], kk=3.0, energy=300.0, cs=2.7,
+                 highres=8.0, lowres=100.0, d_m=kw["diameter"], thres=kw.get("threshold", 7.0),
+                 padding_size=kw["window"], phase_flip=1, overlap=kw["overlap"])
+    ctf = O.make_ctf(p, m.defocus, m.dfdiff, m.dfang, kw["window"])
+    l = geom.l
+    nt_s = 4
+    t0 = time.perf_counter()
+    img = O.preprocess_micrograph(m.image, p, ctf, workers=cores)
+    offx = O.window_offsets(img.shape[1], l, p.overlap)
+    offy = O.window_offsets(img.shape[0], l, p.overlap)
+    W = O.window_spectra(O.split_windows(img, offx, offy, l), p, workers=cores).astype(np.complex64)
+    t_mic = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    T = O.prepare_templates(ds.templates[:nt_s], p, l, ctf, workers=cores)
+    t_tprep = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    TS = O.template_spectra(T, 0.0, p.d_m, workers=cores).astype(np.complex64)
+    t_spec = (time.perf_counter() - t0) / nt_s
+    chk = O.checker(l).astype(np.complex64)
+    TSc = np.conj(TS) * chk[None]
+    nw_s = min(8, W.shape[0])
+    t0 = time.perf_counter()
+    for w in range(nw_s):
+        cc = O._ifft2_unnorm(W[w][None] * TSc, cores).real
+        O.score_maps(cc, p.d_m)
+    t_unit = (time.perf_counter() - t0) / (nw_s * nt_s)
+    nunits = geom.n_angles * geom.n_windows_x * geom.n_windows_y * geom.n_templates
+    t_full = t_mic + t_spec * geom.n_templates * geom.n_angles + t_unit * nunits
+    return {"value": 1.0 / t_full, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": ("oracle restatement, FP32 FFTs on %d host threads: full micrograph "
+                       "preprocessing (%.1f s) + %d templates x 1 angle x %d windows (%.3f s/unit); "
+                       "per-micrograph time extrapolated linearly to %d units (%.0f s)"
+                       % (cores, t_mic, nt_s, nw_s, t_unit, nunits, t_full)),
+            "template_prep_s_per_template": t_tprep / nt_s}
+
+
+# ---------------------------------------------------------------------------
+# our implementation
+# ---------------------------------------------------------------------------
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import gisspa_b200 as G
+    from gisspa_b200 import build
+    if rank == 0:
+        build.build_library()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.set_device(local_rank)
+    ds, kw = make_data(args.workload, seed_offset=rank)
+    m = ds.micrographs[0]
+    ny, nx = m.image.shape
+    ctf = (m.defocus, m.dfdiff, m.dfang)
+    params = params_for(ds, kw)
+    ctx = G.Context(local_rank)
+    t0 = time.perf_counter()
+    ctx.set_templates(params, ds.templates, ctf)
+    t_tmpl = time.perf_counter() - t0
+    geom = ctx.geometry(nx, ny)
+    d_img = torch.from_numpy(m.image).to(f"cuda:{local_rank}")
+    h_img = torch.from_numpy(m.image).pin_memory()
+    torch.cuda.synchronize()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        ctx.search_device(d_img.data_ptr(), nx, ny, ctf)
+    ctx.set_kernel_timing(True)
+    barrier()
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    st0 = ctx.stats()
+    dev_ms = []
+    k_rows = [0.0, 0.0, 0.0, 0.0]
+    npicks = 0
+    for _ in range(args.steps):
+        picks = ctx.search_device(d_img.data_ptr(), nx, ny, ctf)
+        t = ctx.timings()
+        dev_ms.append(t[3])
+        for i in range(4):
+            k_rows[i] += t[4 + i]
+        npicks = len(picks)
+    barrier()
+    clocks = sampler.stop()
+    st1 = ctx.stats()
+    ctx.set_kernel_timing(False)
+    ms_step = sum(dev_ms) / len(dev_ms)
+    # e2e through the public API from pinned host memory
+    barrier()
+    w0 = time.perf_counter()
+    for _ in range(args.steps):
+        picks_e2e = ctx.search(h_img.numpy(), ctf)
+    barrier()
+    e2e_s = (time.perf_counter() - w0) / args.steps
+    times = torch.tensor([ms_step, e2e_s], dtype=torch.float64, device=f"cuda:{local_rank}")
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(times, op=dist.ReduceOp.MAX)
+    ms_step, e2e_s = float(times[0]), float(times[1])
+    if rank != 0:
+        ctx.close()
+        return None
+    peaks, peak_kind = measured_peaks()
+    l = geom.l
+    nw = geom.n_windows_x * geom.n_windows_y
+    na, nt = geom.n_angles, geom.n_templates
+    npairs = (nt + 1) // 2
+    l2 = l * l
+    # dominant kernel: the column pass (inverse FFT along y + score epilogue)
+    # or the row pass (conjugate product + inverse FFT along x), whichever is longer
+    rows_ms, rows_n, cols_ms, cols_n = k_rows
+    bytes_rows = (2 * npairs + 1) * l2 * 8.0       # read P, read W, write R
+    bytes_cols = npairs * l2 * 8.0                 # read R
+    if cols_ms >= rows_ms:
+        kname, kms, kn, kbytes = "column pass (inverse FFT along y + score epilogue)", cols_ms, cols_n, bytes_cols
+    else:
+        kname, kms, kn, kbytes = "row pass (conj product + inverse FFT along x)", rows_ms, rows_n, bytes_rows
+    avg_ms = kms / max(kn, 1)
+    achieved = kbytes / (avg_ms * 1e-3) / 1e9
+    roof = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peaks["hbm_gbs"],
+            "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+            "peak_source": peak_kind, "algorithmic_bytes_per_launch": kbytes,
+            "avg_launch_ms": avg_ms, "launches": kn, "kernel_share_of_step":
+                (rows_ms + cols_ms) / (ms_step * args.steps)}
+    F = micrograph_flops(l, nt, na, nw, nx, ny)
+    sm_mhz = clocks["sm_mhz"] if clocks else 1965.0
+    fp32_peak = 148 * 256 * sm_mhz * 1e6 / 1e12
+    value = world * 1000.0 / ms_step
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": ("full-size single micrograph 5760x4092, 2000 templates 200x200, "
+                                "72 angles, window 720 overlap 200" if args.workload == "full"
+                                else "small micrograph 1024x1024, 50 templates 128x128, 72 angles, "
+                                     "window 512 overlap 128"),
+                   "nx": nx, "ny": ny, "templates": nt, "angles": na, "windows": nw, "l": l,
+                   "units_per_micrograph": na * nw * nt,
+                   "parallelism": "replicas x%d" % world,
+                   "l2": "inputs larger than L2 (template set %.1f GB, pair spectra %.1f GB per angle)"
+                         % (nt * l2 * 4 / 1e9, npairs * l2 * 8 / 1e9)},
+        "e2e": {"value": world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": nx * ny * 4,
+                "d2h_bytes_per_step": 8 + 32 * len(picks_e2e)},
+        "gpu_launches": int(st1.kernel_launches - st0.kernel_launches),
+        "roofline": roof,
+        "roofline_fp32": {"bound": "fp32", "flops_per_micrograph": F,
+                          "achieved": F * (1000.0 / ms_step) / 1e12, "unit": "TFLOP/s",
+                          "peak": fp32_peak, "frac": F * (1000.0 / ms_step) / 1e12 / fp32_peak,
+                          "peak_source": "148 SMs x 256 FLOP/clk x median SM clock under load"},
+        "template_prep_s": t_tmpl,
+        "picks_per_micrograph": npicks,
+        "stage_ms": {"micrograph_prep": float(t[0]), "template_spectra": float(t[1]),
+                     "correlation": float(t[2])},
+        "clocks": clocks,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(ds, kw, geom)
+        except Exception as e:  # reported, not fatal
+            line["cpu_baseline"] = {"error": repr(e)}
+    ctx.close()
+    return line
+
+
+# ---------------------------------------------------------------------------
+# reference arm
+# ---------------------------------------------------------------------------
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    from gisspa_b200 import synth
+    binary = os.path.join(ROOT, "oracle", "_ref", "gisspa_ref")
+    if not os.path.exists(binary):
+        if os.path.isdir("/root/reference"):
+            subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+        if not os.path.exists(binary):
+            return {"impl": "reference", "unavailable": "reference build oracle/_ref/gisspa_ref not present"}
+    window = 768 if args.workload == "full" else 512
+    ds, kw = make_data(args.workload, window=window)
+    work = tempfile.mkdtemp(prefix="gisspa_refbench_")
+    try:
+        m = ds.micrographs[0]
+        ny, nx = m.image.shape
+        nt = ds.templates.shape[0]
+
+        def write(phistep, tag):
+            d = os.path.join(work, tag)
+            ds.params["phistep"] = phistep
+            synth.write_dataset(ds, d)
+            return d
+
+        na_full = int(math.ceil(360.0 / kw["phistep"] - 1e-9))
+        small_step, big_step = 360.0, 90.0          # 1 and 4 angles
+        d1 = write(small_step, "a1")
+        d4 = write(big_step, "a4")
+
+        def run(d):
+            t0 = time.perf_counter()
+            r = subprocess.run([binary, "config"], cwd=d, capture_output=True, text=True, timeout=3600)
+            if r.returncode != 0:
+                raise RuntimeError("reference exited %d: %s" % (r.returncode, r.stderr[-500:]))
+            return time.perf_counter() - t0
+
+        t1 = run(d1)                                  # calibration: fixed cost + 1 angle
+        for _ in range(args.warmup):
+            run(d4)
+        per_angle = []
+        for _ in range(args.steps):
+            t4 = run(d4)
+            per_angle.append(max(t4 - t1, 1e-6) / 3.0)
+        pa = sum(per_angle) / len(per_angle)
+        t_mic = na_full * pa
+        value = 1.0 / t_mic
+        cores = 1
+        sample = ("reference GisSPA binary (its own sources, sm_100a, cuFFT) on the same micrograph "
+                  "and %d templates at window %d; runs of 1 and 4 in-plane angles, per-angle time "
+                  "%.3f s extrapolated linearly to %d angles (%.1f s per micrograph)"
+                  % (nt, window, pa, na_full, t_mic))
+        return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": t_mic * 1000.0, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "impl": "reference",
+                "config": {"workload": "same micrograph and templates, window %d (reference needs "
+                                       "window %% 32 == 0)" % window, "nx": nx, "ny": ny,
+                           "templates": nt, "angles": na_full},
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                                 "sample": sample},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["full", "small"], default="full")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+    else:
+        if world > 1:
+            import datetime
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(local_rank)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                    device_id=torch.device("cuda", local_rank))
+        line = run_ours(args, rank, world, local_rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

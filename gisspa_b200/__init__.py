@@ -55,6 +55,11 @@ class GsGeometry(C.Structure):
                 ("n_angles", C.c_int), ("n_templates", C.c_int)]
 
 
+class GsStats(C.Structure):
+    _fields_ = [("kernel_launches", C.c_ulonglong), ("searches", C.c_ulonglong),
+                ("units", C.c_ulonglong)]
+
+
 UNIT_DTYPE = np.dtype([("score", "<f4"), ("pos", "<i4"), ("peak", "<f4"), ("sigma", "<f4")])
 PICK_DTYPE = np.dtype([("angle_index", "<i4"), ("phi", "<f4"), ("window_x", "<i4"),
                        ("window_y", "<i4"), ("template_index", "<i4"), ("center_x", "<f4"),
@@ -63,7 +68,8 @@ PICK_DTYPE = np.dtype([("angle_index", "<i4"), ("phi", "<f4"), ("window_x", "<i4
 # every entry point declared in include/gisspa.h
 EXPORTS = ("gs_status_string", "gs_version", "gs_params_default", "gs_ctx_create",
            "gs_ctx_destroy", "gs_ctx_last_error", "gs_set_templates", "gs_get_geometry",
-           "gs_search", "gs_search_device", "gs_get_units", "gs_picks_free", "gs_get_timings")
+           "gs_search", "gs_search_device", "gs_get_units", "gs_picks_free", "gs_get_timings",
+           "gs_get_stats", "gs_set_kernel_timing", "gs_set_option")
 
 _lib_handle = None
 
@@ -102,7 +108,10 @@ def load_library(path: Optional[str] = None) -> C.CDLL:
     lib.gs_get_units.argtypes = [vp, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]
     lib.gs_picks_free.argtypes = [C.POINTER(GsPick)]
     lib.gs_picks_free.restype = None
-    lib.gs_get_timings.argtypes = [vp, C.POINTER(C.c_float)]
+    lib.gs_get_timings.argtypes = [vp, C.POINTER(C.c_float), C.c_int]
+    lib.gs_set_kernel_timing.argtypes = [vp, C.c_int]
+    lib.gs_set_option.argtypes = [vp, C.c_int, C.c_int]
+    lib.gs_get_stats.argtypes = [vp, C.POINTER(GsStats)]
     if path is None:
         _lib_handle = lib
     return lib
@@ -216,10 +225,25 @@ class Context:
                     "gs_get_units")
         return out.reshape(shape) if shape is not None else out
 
+    def stats(self) -> GsStats:
+        st = GsStats()
+        self._check(self._lib.gs_get_stats(self._h, C.byref(st)), "gs_get_stats")
+        return st
+
     def timings(self) -> np.ndarray:
-        t = (C.c_float * 4)()
-        self._check(self._lib.gs_get_timings(self._h, t), "gs_get_timings")
+        """[prep, spectra, correlation, total, row-pass ms, row-pass launches,
+        column-pass ms, column-pass launches] of the last search."""
+        t = (C.c_float * 8)()
+        self._check(self._lib.gs_get_timings(self._h, t, 8), "gs_get_timings")
         return np.array(t[:], dtype=np.float64)
+
+    def set_generic_fft(self, enable: bool) -> None:
+        """Force the generic mixed-radix kernels (cross-check of the fast path)."""
+        self._check(self._lib.gs_set_option(self._h, 1, 1 if enable else 0), "gs_set_option")
+
+    def set_kernel_timing(self, enable: bool) -> None:
+        self._check(self._lib.gs_set_kernel_timing(self._h, 1 if enable else 0),
+                    "gs_set_kernel_timing")
 
 
 def run_config(config_path: str, device: Optional[int] = None, return_units: bool = False):

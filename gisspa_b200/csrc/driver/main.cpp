@@ -186,8 +186,8 @@ int main(int argc, char** argv) {
                     eul.az[pk.template_index], pk.phi, pk.center_x, pk.center_y, pk.score);
         }
         gs_picks_free(picks);
-        float ms[4];
-        gs_get_timings(ctx, ms);
+        float ms[GS_TIMING_COUNT];
+        gs_get_timings(ctx, ms, GS_TIMING_COUNT);
         printf("Image %d: %zu picks, %.1f ms (preprocess %.1f, template spectra %.1f, correlation %.1f)\n", n, np,
                ms[3], ms[0], ms[1], ms[2]);
         printf("------------------------Image %d finished--------------------------------\n", n);

@@ -38,14 +38,14 @@ __device__ __forceinline__ float2 twiddle(const float2* tw, int idx, bool inv) {
 }
 
 template <bool kInv>
-__device__ __forceinline__ void dft2(float2& a0, float2& a1) {
+__host__ __device__ __forceinline__ void dft2(float2& a0, float2& a1) {
     float2 t = a0;
     a0 = cadd(t, a1);
     a1 = csub(t, a1);
 }
 
 template <bool kInv>
-__device__ __forceinline__ void dft3(float2& a0, float2& a1, float2& a2) {
+__host__ __device__ __forceinline__ void dft3(float2& a0, float2& a1, float2& a2) {
     const float s = 0.86602540378443864676f;
     float2 t1 = cadd(a1, a2);
     float2 t2 = make_float2(a0.x - 0.5f * t1.x, a0.y - 0.5f * t1.y);
@@ -57,7 +57,7 @@ __device__ __forceinline__ void dft3(float2& a0, float2& a1, float2& a2) {
 }
 
 template <bool kInv>
-__device__ __forceinline__ void dft4(float2& a0, float2& a1, float2& a2, float2& a3) {
+__host__ __device__ __forceinline__ void dft4(float2& a0, float2& a1, float2& a2, float2& a3) {
     float2 s02 = cadd(a0, a2), d02 = csub(a0, a2);
     float2 s13 = cadd(a1, a3), d13 = mul_mi<kInv>(csub(a1, a3));
     a0 = cadd(s02, s13);
@@ -67,7 +67,7 @@ __device__ __forceinline__ void dft4(float2& a0, float2& a1, float2& a2, float2&
 }
 
 template <bool kInv>
-__device__ __forceinline__ void dft5(float2& a0, float2& a1, float2& a2, float2& a3, float2& a4) {
+__host__ __device__ __forceinline__ void dft5(float2& a0, float2& a1, float2& a2, float2& a3, float2& a4) {
     const float c1 = 0.30901699437494742410f;   // cos(2 pi / 5)
     const float c2 = -0.80901699437494742410f;  // cos(4 pi / 5)
     const float s1 = 0.95105651629515357212f;   // sin(2 pi / 5)
@@ -89,7 +89,7 @@ __device__ __forceinline__ void dft5(float2& a0, float2& a1, float2& a2, float2&
 }
 
 template <bool kInv>
-__device__ __forceinline__ void dft8(float2* a) {
+__host__ __device__ __forceinline__ void dft8(float2* a) {
     const float h = 0.70710678118654752440f;
     // even / odd radix-4 halves
     float2 e0 = a[0], e1 = a[2], e2 = a[4], e3 = a[6];

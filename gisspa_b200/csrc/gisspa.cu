@@ -6,6 +6,7 @@
 // micrograph preprocessing, window spectra, then for every in-plane angle the
 // template-pair spectra and, for every window, the fused correlation passes.
 #include "gisspa.h"
+#include "fastfft.cuh"
 #include "kernels.cuh"
 
 #include <algorithm>
@@ -51,7 +52,11 @@ struct gs_ctx {
     // last search
     int last_na = 0, last_nw = 0, last_nt = 0;
     bool have_units = false;
-    float timings[4] = {0, 0, 0, 0};
+    float timings[GS_TIMING_COUNT] = {0, 0, 0, 0, 0, 0, 0, 0};
+    bool kernel_timing = false;
+    bool generic_fft = false;
+    std::vector<cudaEvent_t> kev;  // pool of events for per-kernel timing
+    gs_stats counters{0, 0, 0};
 };
 
 namespace {
@@ -74,9 +79,9 @@ int set_err(gs_ctx* c, int code, const char* fmt, ...) {
         if (e_ != cudaSuccess) return set_err(ctx, GS_ERR_CUDA, "%s: %s", #expr, cudaGetErrorString(e_)); \
     } while (0)
 #define CKL() CK(cudaGetLastError())
-#define TRY(expr)                  \
+#define TRY(...)                   \
     do {                           \
-        int s_ = (expr);           \
+        int s_ = (__VA_ARGS__);    \
         if (s_ != GS_OK) return s_; \
     } while (0)
 
@@ -164,8 +169,44 @@ int run_fft(gs_ctx* ctx, int n, VecGeom g, int nimg, IO io, int max_tile = 16) {
     CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 grid((unsigned)((g.nvec + tile - 1) / tile), (unsigned)nimg);
     kern<<<grid, kFftThreads, smem, ctx->stream>>>(pl->d, g, (int)tile, io);
+    ++ctx->counters.kernel_launches;
     CKL();
     return GS_OK;
+}
+
+// Specialised l = 16 * N2 kernels (fastfft.cuh) exist for these sizes.
+bool fast_ok(const gs_ctx* ctx, int l) {
+    if (ctx->generic_fft || l % 16) return false;
+    const int n2 = l / 16;
+    return n2 == 32 || n2 == 45 || n2 == 48;
+}
+
+template <int N2, bool kInv, bool kCols, class IO>
+int launch_fast_n2(gs_ctx* ctx, const float2* tw, int nimg, IO io) {
+    using F = Fast16<N2>;
+    auto kern = k_fft16<N2, kInv, kCols, IO>;
+    const size_t smem = F::smem_bytes();
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid(N2, (unsigned)nimg);
+    kern<<<grid, F::kThreads, smem, ctx->stream>>>(tw, io);
+    ++ctx->counters.kernel_launches;
+    CKL();
+    return GS_OK;
+}
+
+// Batched l x l transform along rows (kCols = false) or columns of nimg
+// images through the specialised kernels; fast_ok(l) must hold.
+template <bool kInv, bool kCols, class IO>
+int run_fast(gs_ctx* ctx, int l, int nimg, IO io) {
+    FftPlan* pl = nullptr;
+    TRY(get_plan(ctx, l, &pl));
+    if (nimg > 65535) return set_err(ctx, GS_ERR_UNSUPPORTED, "too many images in one FFT batch (%d)", nimg);
+    switch (l / 16) {
+        case 32: return launch_fast_n2<32, kInv, kCols>(ctx, pl->tw, nimg, io);
+        case 45: return launch_fast_n2<45, kInv, kCols>(ctx, pl->tw, nimg, io);
+        case 48: return launch_fast_n2<48, kInv, kCols>(ctx, pl->tw, nimg, io);
+        default: return set_err(ctx, GS_ERR_UNSUPPORTED, "no specialised FFT for %d", l);
+    }
 }
 
 // Row / column geometry of a batch of row-major h x w images (vectors of
@@ -301,6 +342,7 @@ int gs_ctx_destroy(gs_ctx* ctx) {
                     &ctx->off, &ctx->win, &ctx->wsum, &ctx->winv, &ctx->tspec, &ctx->scratch, &ctx->pstats,
                     &ctx->coef, &ctx->acc, &ctx->units, &ctx->picks, &ctx->count};
     for (DBuf* b : bufs) free_buf(*b);
+    for (cudaEvent_t e : ctx->kev) cudaEventDestroy(e);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return GS_OK;
@@ -359,6 +401,7 @@ int gs_set_templates(gs_ctx* ctx, const gs_params* p, const float* host_template
         wc.kk = p->kk; wc.a = p->a; wc.b = p->b; wc.b2 = p->b2;
         wc.bf = p->bfactor; wc.bf2 = p->bfactor2; wc.bf3 = p->bfactor3;
         k_weight_map<<<blocks_for((long long)l2, 256), 256, 0, ctx->stream>>>(P<float>(wmap), l, wc, c0);
+        ++ctx->counters.kernel_launches;
         if ((st = (cudaGetLastError() == cudaSuccess ? GS_OK : set_err(ctx, GS_ERR_CUDA, "k_weight_map")))) break;
         for (int c0i = 0; c0i < n && st == GS_OK; c0i += chunk) {
             const int nc = std::min(chunk, n - c0i);
@@ -366,21 +409,36 @@ int gs_set_templates(gs_ctx* ctx, const gs_params* p, const float* host_template
                                             sizeof(float) * (size_t)tx * ty * nc, cudaMemcpyHostToDevice, ctx->stream);
             if (e != cudaSuccess) { st = set_err(ctx, GS_ERR_CUDA, "template upload: %s", cudaGetErrorString(e)); break; }
             k_tmpl_pad_edge<<<nc, 256, 0, ctx->stream>>>(P<float>(raw), tx, ty, l, P<float2>(F));
+            ++ctx->counters.kernel_launches;
             if (cudaGetLastError() != cudaSuccess) { st = set_err(ctx, GS_ERR_CUDA, "k_tmpl_pad_edge"); break; }
-            if ((st = run_fft<false>(ctx, l, rows_of(l, l), nc, IoComplex{P<float2>(F), 1.0f}))) break;
-            if ((st = run_fft<false>(ctx, l, cols_of(l, l), nc, IoComplex{P<float2>(F), 1.0f / (float)l2}))) break;
+            if (fast_ok(ctx, l)) {
+                if ((st = run_fast<false, false>(ctx, l, nc, F16Complex<false>{P<float2>(F), l, (long long)l2, 1.0f}))) break;
+                if ((st = run_fast<false, true>(ctx, l, nc, F16Complex<true>{P<float2>(F), l, (long long)l2, 1.0f / (float)l2}))) break;
+            } else {
+                if ((st = run_fft<false>(ctx, l, rows_of(l, l), nc, IoComplex{P<float2>(F), 1.0f}))) break;
+                if ((st = run_fft<false>(ctx, l, cols_of(l, l), nc, IoComplex{P<float2>(F), 1.0f / (float)l2}))) break;
+            }
             const size_t shs = (size_t)(l / 2) * (sizeof(double) + sizeof(unsigned));
             if (shs > kMaxSmem) { st = set_err(ctx, GS_ERR_UNSUPPORTED, "window too large"); break; }
             cudaFuncSetAttribute(k_tmpl_shells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shs);
             k_tmpl_shells<<<nc, 256, shs, ctx->stream>>>(P<float2>(F), l, P<float>(div));
+            ++ctx->counters.kernel_launches;
             cudaMemsetAsync(P<double>(sumsq), 0, sizeof(double) * 2 * nc, ctx->stream);
             dim3 g(blocks_for((long long)l2, 256, 64), nc);
             k_tmpl_apply<<<g, 256, 0, ctx->stream>>>(P<float2>(F), l, P<float>(div), P<float>(wmap), P<double>(sumsq));
+            ++ctx->counters.kernel_launches;
             k_inv_amp_norm<<<blocks_for(nc, 128), 128, 0, ctx->stream>>>(P<double>(sumsq), nc, P<double>(inv));
+            ++ctx->counters.kernel_launches;
             if (cudaGetLastError() != cudaSuccess) { st = set_err(ctx, GS_ERR_CUDA, "template weighting"); break; }
-            if ((st = run_fft<true>(ctx, l, rows_of(l, l), nc, IoScaleIn{P<float2>(F), P<double>(inv)}))) break;
-            if ((st = run_fft<true>(ctx, l, cols_of(l, l), nc,
-                                    IoRealOut{P<float2>(F), P<float>(ctx->tmpl) + (size_t)c0i * l2, 1.0f}))) break;
+            if (fast_ok(ctx, l)) {
+                if ((st = run_fast<true, false>(ctx, l, nc, F16ScaleIn<false>{P<float2>(F), P<double>(inv), l, (long long)l2}))) break;
+                if ((st = run_fast<true, true>(ctx, l, nc, F16RealOut<true>{P<float2>(F), P<float>(ctx->tmpl) + (size_t)c0i * l2,
+                                                                            l, (long long)l2}))) break;
+            } else {
+                if ((st = run_fft<true>(ctx, l, rows_of(l, l), nc, IoScaleIn{P<float2>(F), P<double>(inv)}))) break;
+                if ((st = run_fft<true>(ctx, l, cols_of(l, l), nc,
+                                        IoRealOut{P<float2>(F), P<float>(ctx->tmpl) + (size_t)c0i * l2, 1.0f}))) break;
+            }
         }
         if (st) break;
         cudaError_t e = cudaStreamSynchronize(ctx->stream);
@@ -437,9 +495,12 @@ static int search_impl(gs_ctx* ctx, const float* d_mic, int nx, int ny, const gs
     float* q1 = P<float>(ctx->q);
     float* q2 = q1 + npix;
     k_mic_quot<<<blocks_for(npix, 256), 256, 0, ctx->stream>>>(d_mic, npix, nx, ny, q1, q2);
+    ++ctx->counters.kernel_launches;
     k_mic_seq<<<1, 32, 0, ctx->stream>>>(q1, q2, npix, P<MicStats>(ctx->stats));
+    ++ctx->counters.kernel_launches;
     k_mic_clamp<<<blocks_for(npix, 256), 256, 0, ctx->stream>>>(d_mic, npix, P<MicStats>(ctx->stats), p.invert,
                                                                  P<float2>(ctx->cimg));
+    ++ctx->counters.kernel_launches;
     CKL();
     float2* C = P<float2>(ctx->cimg);
     TRY(run_fft<false>(ctx, nx, rows_of(nx, ny), 1, IoComplex{C, 1.0f}));
@@ -453,6 +514,7 @@ static int search_impl(gs_ctx* ctx, const float* d_mic, int nx, int ny, const gs
         CK(cudaFuncSetAttribute(k_mic_flip_shells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shs));
         const unsigned nb = (unsigned)std::min(ny, 296);
         k_mic_flip_shells<<<nb, 256, shs, ctx->stream>>>(C, nx, ny, cm, P<double>(ctx->ra), P<unsigned>(ctx->rb));
+        ++ctx->counters.kernel_launches;
         MicWhitenConsts w;
         const int L = std::max(nx, ny);
         w.apix = p.apix;
@@ -463,8 +525,10 @@ static int search_impl(gs_ctx* ctx, const float* d_mic, int nx, int ny, const gs
         w.bf = p.bfactor; w.bf2 = p.bfactor2; w.bf3 = p.bfactor3;
         k_mic_whiten<<<blocks_for(npix, 256), 256, 0, ctx->stream>>>(C, nx, ny, cm, w, P<double>(ctx->ra),
                                                                       P<unsigned>(ctx->rb));
+        ++ctx->counters.kernel_launches;
     } else {
         k_set_dc_zero<<<1, 1, 0, ctx->stream>>>(C);
+        ++ctx->counters.kernel_launches;
     }
     CKL();
     TRY(run_fft<true>(ctx, ny, cols_of(nx, ny), 1, IoComplex{C, 1.0f}));
@@ -482,19 +546,28 @@ static int search_impl(gs_ctx* ctx, const float* d_mic, int nx, int ny, const gs
     {
         dim3 g(blocks_for(l2, 256, 256), nw);
         k_extract_windows<<<g, 256, 0, ctx->stream>>>(P<float>(ctx->img), nx, ny, d_offx, d_offy, bx, l, W);
+        ++ctx->counters.kernel_launches;
         CKL();
     }
-    TRY(run_fft<false>(ctx, l, rows_of(l, l), nw, IoComplex{W, 1.0f}));
-    TRY(run_fft<false>(ctx, l, cols_of(l, l), nw, IoComplex{W, (float)(1.0 / (double)l2)}));
+    if (fast_ok(ctx, l)) {
+        TRY(run_fast<false, false>(ctx, l, nw, F16Complex<false>{W, l, l2, 1.0f}));
+        TRY(run_fast<false, true>(ctx, l, nw, F16Complex<true>{W, l, l2, (float)(1.0 / (double)l2)}));
+    } else {
+        TRY(run_fft<false>(ctx, l, rows_of(l, l), nw, IoComplex{W, 1.0f}));
+        TRY(run_fft<false>(ctx, l, cols_of(l, l), nw, IoComplex{W, (float)(1.0 / (double)l2)}));
+    }
     if (p.phase_flip == 1) {
         TRY(ensure(ctx, ctx->wsum, sizeof(double) * 2 * nw));
         TRY(ensure(ctx, ctx->winv, sizeof(double) * nw));
         CK(cudaMemsetAsync(ctx->wsum.p, 0, sizeof(double) * 2 * nw, ctx->stream));
         dim3 g(blocks_for(l2 / 2, 256, 64), nw);
         k_win_sumsq<<<g, 256, 0, ctx->stream>>>(W, l, P<double>(ctx->wsum));
+        ++ctx->counters.kernel_launches;
         k_inv_amp_norm<<<blocks_for(nw, 128), 128, 0, ctx->stream>>>(P<double>(ctx->wsum), nw, P<double>(ctx->winv));
+        ++ctx->counters.kernel_launches;
         dim3 g2(blocks_for(l2, 256, 256), nw);
         k_scale_images<<<g2, 256, 0, ctx->stream>>>(W, l2, P<double>(ctx->winv));
+        ++ctx->counters.kernel_launches;
         CKL();
     }
     CK(cudaEventRecord(ev[1], ctx->stream));
@@ -513,7 +586,15 @@ static int search_impl(gs_ctx* ctx, const float* d_mic, int nx, int ny, const gs
     const float q_lo = p.d_m / 4.0f;
     const float q_hi = (float)l - q_lo;
     const float sgn = ((l / 2) % 2 == 0) ? 1.0f : -1.0f;
-    float ms_spec = 0.0f, ms_corr = 0.0f;
+    float ms_spec = 0.0f, ms_corr = 0.0f, k1ms = 0.0f, k2ms = 0.0f;
+    long long k1n = 0, k2n = 0;
+    if (ctx->kernel_timing && (int)ctx->kev.size() < 4 * nw) {
+        while ((int)ctx->kev.size() < 4 * nw) {
+            cudaEvent_t e;
+            CK(cudaEventCreate(&e));
+            ctx->kev.push_back(e);
+        }
+    }
     cudaEvent_t ea, eb, ec;
     CK(cudaEventCreate(&ea));
     CK(cudaEventCreate(&eb));
@@ -529,21 +610,42 @@ static int search_impl(gs_ctx* ctx, const float* d_mic, int nx, int ny, const gs
             dim3 g(blocks_for(l2, 256, 32), Np);
             k_pair_rotate<<<g, 256, 0, ctx->stream>>>(P<float>(ctx->tmpl), N, l, cose, sine, p.d_m, TS,
                                                       P<double>(ctx->pstats));
+            ++ctx->counters.kernel_launches;
             k_pair_coef<<<blocks_for(Np, 128), 128, 0, ctx->stream>>>(P<double>(ctx->pstats), N, l,
                                                                        P<float4>(ctx->coef));
+            ++ctx->counters.kernel_launches;
             CKL();
         }
-        TRY(run_fft<false>(ctx, l, rows_of(l, l), Np, IoPairNorm{TS, P<float4>(ctx->coef), l2}));
-        TRY(run_fft<false>(ctx, l, cols_of(l, l), Np, IoComplex{TS, (float)(1.0 / (double)l2)}));
+        if (fast_ok(ctx, l)) {
+            TRY(run_fast<false, false>(ctx, l, Np, F16PairNorm{TS, P<float4>(ctx->coef), l, l2}));
+            TRY(run_fast<false, true>(ctx, l, Np, F16Complex<true>{TS, l, l2, (float)(1.0 / (double)l2)}));
+        } else {
+            TRY(run_fft<false>(ctx, l, rows_of(l, l), Np, IoPairNorm{TS, P<float4>(ctx->coef), l2}));
+            TRY(run_fft<false>(ctx, l, cols_of(l, l), Np, IoComplex{TS, (float)(1.0 / (double)l2)}));
+        }
         CK(cudaEventRecord(eb, ctx->stream));
         for (int w = 0; w < nw; ++w) {
             CK(cudaMemsetAsync(acc, 0, sizeof(UnitAcc) * N, ctx->stream));
-            TRY(run_fft<true>(ctx, l, rows_of(l, l), Np, IoPass1{W + (size_t)w * l2, TS, R, l2}));
-            IoPass2 io2;
-            io2.R = R; io2.acc = acc; io2.l = l; io2.ntmpl = N; io2.q_lo = q_lo; io2.q_hi = q_hi; io2.sgn = sgn;
-            TRY(run_fft<true>(ctx, l, cols_of(l, l), Np, io2));
+            const bool fast = fast_ok(ctx, l);
+            if (ctx->kernel_timing) CK(cudaEventRecord(ctx->kev[4 * w + 0], ctx->stream));
+            if (fast) TRY(run_fast<true, false>(ctx, l, Np, F16Pass1{W + (size_t)w * l2, TS, R, l, l2}));
+            else TRY(run_fft<true>(ctx, l, rows_of(l, l), Np, IoPass1{W + (size_t)w * l2, TS, R, l2}));
+            if (ctx->kernel_timing) CK(cudaEventRecord(ctx->kev[4 * w + 1], ctx->stream));
+            if (ctx->kernel_timing) CK(cudaEventRecord(ctx->kev[4 * w + 2], ctx->stream));
+            if (fast) {
+                F16Pass2 io2;
+                io2.R = R; io2.acc = acc; io2.L = l; io2.ntmpl = N; io2.L2 = l2;
+                io2.q_lo = q_lo; io2.q_hi = q_hi; io2.sgn = sgn;
+                TRY(run_fast<true, true>(ctx, l, Np, io2));
+            } else {
+                IoPass2 io2;
+                io2.R = R; io2.acc = acc; io2.l = l; io2.ntmpl = N; io2.q_lo = q_lo; io2.q_hi = q_hi; io2.sgn = sgn;
+                TRY(run_fft<true>(ctx, l, cols_of(l, l), Np, io2));
+            }
+            if (ctx->kernel_timing) CK(cudaEventRecord(ctx->kev[4 * w + 3], ctx->stream));
             k_finalize<<<blocks_for(N, 128), 128, 0, ctx->stream>>>(acc, N, l,
                                                                     units + ((size_t)ai * nw + w) * N);
+            ++ctx->counters.kernel_launches;
             CKL();
         }
         CK(cudaEventRecord(ec, ctx->stream));
@@ -553,6 +655,17 @@ static int search_impl(gs_ctx* ctx, const float* d_mic, int nx, int ny, const gs
         cudaEventElapsedTime(&t2, eb, ec);
         ms_spec += t1;
         ms_corr += t2;
+        if (ctx->kernel_timing) {
+            for (int w = 0; w < nw; ++w) {
+                float a = 0, b = 0;
+                cudaEventElapsedTime(&a, ctx->kev[4 * w + 0], ctx->kev[4 * w + 1]);
+                cudaEventElapsedTime(&b, ctx->kev[4 * w + 2], ctx->kev[4 * w + 3]);
+                k1ms += a;
+                k2ms += b;
+            }
+            k1n += nw;
+            k2n += nw;
+        }
     }
     ctx->last_na = na;
     ctx->last_nw = nw;
@@ -567,6 +680,7 @@ static int search_impl(gs_ctx* ctx, const float* d_mic, int nx, int ny, const gs
         k_compact<<<blocks_for(total_units, 256), 256, 0, ctx->stream>>>(
             units, total_units, nw, N, bx, d_offx, d_offy, l, p.d_m, nx, ny, p.thres, P<PickDev>(ctx->picks),
             P<unsigned long long>(ctx->count), total_units);
+        ++ctx->counters.kernel_launches;
         CKL();
     }
     unsigned long long cnt = 0;
@@ -606,6 +720,12 @@ static int search_impl(gs_ctx* ctx, const float* d_mic, int nx, int ny, const gs
     ctx->timings[1] = ms_spec;
     ctx->timings[2] = ms_corr;
     ctx->timings[3] = t_tot;
+    ctx->timings[4] = k1ms;
+    ctx->timings[5] = (float)k1n;
+    ctx->timings[6] = k2ms;
+    ctx->timings[7] = (float)k2n;
+    ctx->counters.searches += 1;
+    ctx->counters.units += (unsigned long long)total_units;
     return GS_OK;
 }
 
@@ -649,9 +769,29 @@ int gs_get_units(gs_ctx* ctx, gs_unit* host_out, size_t cap, size_t* n_out) {
 
 void gs_picks_free(gs_pick* p) { free(p); }
 
-int gs_get_timings(gs_ctx* ctx, float* ms4) {
-    if (!ctx || !ms4) return GS_ERR_ARG;
-    for (int i = 0; i < 4; ++i) ms4[i] = ctx->timings[i];
+int gs_get_stats(gs_ctx* ctx, gs_stats* out) {
+    if (!ctx || !out) return GS_ERR_ARG;
+    *out = ctx->counters;
+    return GS_OK;
+}
+
+int gs_get_timings(gs_ctx* ctx, float* out, int n) {
+    if (!ctx || !out || n < 0) return GS_ERR_ARG;
+    for (int i = 0; i < n && i < GS_TIMING_COUNT; ++i) out[i] = ctx->timings[i];
+    return GS_OK;
+}
+
+int gs_set_option(gs_ctx* ctx, int option, int value) {
+    if (!ctx) return GS_ERR_ARG;
+    switch (option) {
+        case GS_OPT_GENERIC_FFT: ctx->generic_fft = value != 0; return GS_OK;
+        default: return set_err(ctx, GS_ERR_ARG, "unknown option %d", option);
+    }
+}
+
+int gs_set_kernel_timing(gs_ctx* ctx, int enable) {
+    if (!ctx) return GS_ERR_ARG;
+    ctx->kernel_timing = enable != 0;
     return GS_OK;
 }
 

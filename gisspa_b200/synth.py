@@ -67,13 +67,44 @@ def projected_blobs(den: Density, alt: float, az: float) -> Tuple[np.ndarray, np
 
 
 def render_gaussians(centers_xy: np.ndarray, amps: np.ndarray, sigmas: np.ndarray,
-                     size: int) -> np.ndarray:
+                     size: int, dtype=np.float64) -> np.ndarray:
     """Separable render of sum_b amp_b exp(-|p - c_b|^2 / (2 s_b^2)) on a size^2
     grid whose centre pixel (size//2, size//2) is the origin."""
     g = np.arange(size, dtype=np.float64) - size // 2
     gx = np.exp(-((g[None, :] - centers_xy[:, 0:1]) ** 2) / (2 * sigmas[:, None] ** 2))
     gy = np.exp(-((g[None, :] - centers_xy[:, 1:2]) ** 2) / (2 * sigmas[:, None] ** 2))
-    return gy.T @ (amps[:, None] * gx)
+    return (gy.T.astype(dtype) @ (amps[:, None] * gx).astype(dtype)).astype(np.float64)
+
+
+def render_gaussians_batch(centers_xy: np.ndarray, amps: np.ndarray, sigmas: np.ndarray,
+                           size: int) -> np.ndarray:
+    """float32 batched version of :func:`render_gaussians` on CPU threads:
+    centers_xy (K, B, 2), amps (K, B) -> (K, size, size)."""
+    import torch
+    g = torch.arange(size, dtype=torch.float32) - size // 2
+    c = torch.from_numpy(np.ascontiguousarray(centers_xy, dtype=np.float32))
+    a = torch.from_numpy(np.ascontiguousarray(amps, dtype=np.float32))
+    s2 = torch.from_numpy(np.asarray(2.0 * sigmas ** 2, dtype=np.float32))[None, :, None]
+    gx = torch.exp(-((g[None, None, :] - c[:, :, 0:1]) ** 2) / s2) * a[:, :, None]
+    gy = torch.exp(-((g[None, None, :] - c[:, :, 1:2]) ** 2) / s2)
+    return torch.bmm(gy.transpose(1, 2), gx).numpy()
+
+
+def jittered_grid(rng: np.random.Generator, nx: int, ny: int, count: int, margin: float,
+                  min_dist: float) -> List[Tuple[int, int]]:
+    """``count`` positions >= ``margin`` from the edges and >= ``min_dist``
+    apart: one per cell of a grid of pitch min_dist + 2 j, jittered by +-j."""
+    jit = 8
+    pitch = int(math.ceil(min_dist)) + 2 * jit
+    xs = np.arange(int(math.ceil(margin)) + jit, nx - int(math.ceil(margin)) - jit, pitch)
+    ys = np.arange(int(math.ceil(margin)) + jit, ny - int(math.ceil(margin)) - jit, pitch)
+    cells = [(x, y) for y in ys for x in xs]
+    pick = rng.permutation(len(cells))[:count]
+    out = []
+    for k in pick:
+        x, y = cells[k]
+        out.append((int(x + rng.integers(-jit, jit + 1)), int(y + rng.integers(-jit, jit + 1))))
+    return out
 
 
 def ctf_value(size: int, apix: float, defocus_um: float, dfdiff_um: float, dfang_deg: float,
@@ -154,17 +185,26 @@ def make_dataset(seed: int, *, nx: int, ny: int, n_templates: int, tsize: int,
                  sizes: Optional[Sequence[Tuple[int, int]]] = None,
                  hot_pixels: int = 0, threshold: float = 7.0, phase_flip: int = 1,
                  invert: int = 0, highres: float = 8.0, lowres: float = 100.0,
-                 kk: float = 3.0) -> Dataset:
+                 kk: float = 3.0, fast: bool = False) -> Dataset:
+    """``fast`` renders in float32 with a particle box of 1.5 x the template
+    size (instead of the next power of two); used for the large workloads."""
     rng = np.random.default_rng(seed)
     den = make_density(rng, n_blobs, ball_radius)
     views = random_views(rng, n_templates)
     tmpl = np.empty((n_templates, tsize, tsize), dtype=np.float32)
-    for k in range(n_templates):
-        c, a = projected_blobs(den, float(views[k, 0]), float(views[k, 1]))
-        tmpl[k] = render_gaussians(c, a, den.sigmas, tsize).astype(np.float32)
+    if fast:
+        for k0 in range(0, n_templates, 250):
+            proj = [projected_blobs(den, float(views[k, 0]), float(views[k, 1]))
+                    for k in range(k0, min(n_templates, k0 + 250))]
+            tmpl[k0:k0 + len(proj)] = render_gaussians_batch(
+                np.stack([c for c, _ in proj]), np.stack([a for _, a in proj]), den.sigmas, tsize)
+    else:
+        for k in range(n_templates):
+            c, a = projected_blobs(den, float(views[k, 0]), float(views[k, 1]))
+            tmpl[k] = render_gaussians(c, a, den.sigmas, tsize).astype(np.float32)
     n_angles = int(math.ceil(360.0 / phistep - 1e-9))
     mics: List[Micrograph] = []
-    box = int(2 ** math.ceil(math.log2(tsize * 1.5)))
+    box = (int(math.ceil(tsize * 0.75)) * 2) if fast else int(2 ** math.ceil(math.log2(tsize * 1.5)))
     for m in range(n_micrographs):
         mx, my = (sizes[m] if sizes is not None else (nx, ny))
         img = coloured_noise(rng, my, mx, noise_alpha)
@@ -172,20 +212,36 @@ def make_dataset(seed: int, *, nx: int, ny: int, n_templates: int, tsize: int,
         dd = float(rng.uniform(0.0, astig_A)) / 2.0 / 1e4 if astig_A > 0 else 0.0
         da = float(rng.uniform(0.0, 180.0)) if astig_A > 0 else 0.0
         ctf = ctf_value(box, apix, d0, dd, da)
-        pts = place_particles(rng, mx, my, n_particles, diameter + box // 2, diameter)
+        if fast:
+            pts = jittered_grid(rng, mx, my, n_particles, diameter + box // 2, 2 * ball_radius)
+        else:
+            pts = place_particles(rng, mx, my, n_particles, diameter + box // 2, diameter)
         parts: List[Particle] = []
         sig = np.zeros((my, mx))
         disc_vals = []
-        for (x, y) in pts:
-            J = int(rng.integers(0, n_templates))
-            ai = int(rng.integers(0, n_angles))
-            e = math.radians(ai * phistep)
-            c, s = math.cos(e), math.sin(e)
-            q, a = projected_blobs(den, float(views[J, 0]), float(views[J, 1]))
-            # the search rotates template J by e with source (c x + s y, -s x + c y):
-            # the matching particle has its blob centres at (c qx - s qy, s qx + c qy)
-            rc = np.stack([c * q[:, 0] - s * q[:, 1], s * q[:, 0] + c * q[:, 1]], axis=1)
-            p = render_gaussians(rc, a, den.sigmas, box)
+        choice = [(int(rng.integers(0, n_templates)), int(rng.integers(0, n_angles))) for _ in pts]
+        rendered = None
+        if fast and pts:
+            cs_, as_ = [], []
+            for (J, ai) in choice:
+                e = math.radians(ai * phistep)
+                c, s = math.cos(e), math.sin(e)
+                q, a = projected_blobs(den, float(views[J, 0]), float(views[J, 1]))
+                cs_.append(np.stack([c * q[:, 0] - s * q[:, 1], s * q[:, 0] + c * q[:, 1]], axis=1))
+                as_.append(a)
+            rendered = render_gaussians_batch(np.stack(cs_), np.stack(as_), den.sigmas, box)
+        for idx, (x, y) in enumerate(pts):
+            J, ai = choice[idx]
+            if rendered is not None:
+                p = rendered[idx].astype(np.float64)
+            else:
+                e = math.radians(ai * phistep)
+                c, s = math.cos(e), math.sin(e)
+                q, a = projected_blobs(den, float(views[J, 0]), float(views[J, 1]))
+                # the search rotates template J by e with source (c x + s y, -s x + c y):
+                # the matching particle has its blob centres at (c qx - s qy, s qx + c qy)
+                rc = np.stack([c * q[:, 0] - s * q[:, 1], s * q[:, 0] + c * q[:, 1]], axis=1)
+                p = render_gaussians(rc, a, den.sigmas, box)
             p = np.fft.ifft2(np.fft.fft2(np.fft.ifftshift(p)) * ctf).real
             p = np.fft.fftshift(p)
             x0, y0 = x - box // 2, y - box // 2
@@ -232,7 +288,7 @@ def config_full(seed: int = 1, window: int = 720) -> Dict[str, object]:
     return dict(seed=seed, nx=5760, ny=4092, n_templates=2000, tsize=200, n_particles=400,
                 snr=0.03, n_blobs=800, ball_radius=90.0, phistep=5.0, diameter=190.0,
                 window=window, overlap=200, defocus=(0.8, 2.5), astig_A=500.0,
-                noise_alpha=0.5, threshold=7.0)
+                noise_alpha=0.5, threshold=7.0, fast=True)
 
 
 def write_dataset(ds: Dataset, outdir: str, extra: Optional[Dict[str, object]] = None,

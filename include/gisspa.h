@@ -148,10 +148,35 @@ int gs_get_units(struct gs_ctx* ctx, gs_unit* host_out, size_t cap, size_t* n_ou
 
 void gs_picks_free(gs_pick* picks);
 
-/* Timings of the last search, milliseconds, measured with CUDA events on the
- * context's stream: [0] micrograph preprocessing, [1] template spectra (all
- * angles), [2] correlation passes (all angles), [3] total. */
-int gs_get_timings(struct gs_ctx* ctx, float* ms4);
+/* Timings of the last search, measured with CUDA events on the context's
+ * stream (no reference counterpart; the reference prints whole seconds,
+ * main.cu:1271-1272).  Fills min(n, GS_TIMING_COUNT) entries:
+ *  [0] micrograph preprocessing ms   [1] template spectra ms (all angles)
+ *  [2] correlation ms (all angles)    [3] total ms
+ *  [4] row-pass kernel ms (sum)       [5] row-pass launches
+ *  [6] column-pass kernel ms (sum)    [7] column-pass launches
+ * Entries 4-7 are filled only while per-kernel timing is enabled. */
+#define GS_TIMING_COUNT 8
+int gs_get_timings(struct gs_ctx* ctx, float* out, int n);
+
+/* Enable (1) or disable (0) per-kernel event timing of the correlation
+ * passes; it adds two events per launch. */
+int gs_set_kernel_timing(struct gs_ctx* ctx, int enable);
+
+/* Tuning / cross-check options (no reference counterpart).
+ * GS_OPT_GENERIC_FFT: 1 = always use the generic mixed-radix kernels, 0 =
+ * use the specialised l = 16*N2 kernels where they exist (default). */
+#define GS_OPT_GENERIC_FFT 1
+int gs_set_option(struct gs_ctx* ctx, int option, int value);
+
+/* Counters of this context since creation (no reference counterpart; the
+ * reference reports only its wall time, main.cu:1271-1272). */
+typedef struct gs_stats {
+    unsigned long long kernel_launches; /* kernels this library launched */
+    unsigned long long searches;        /* completed gs_search* calls */
+    unsigned long long units;           /* (angle, window, template) units scored */
+} gs_stats;
+int gs_get_stats(struct gs_ctx* ctx, gs_stats* out);
 
 #ifdef __cplusplus
 }
