@@ -66,9 +66,11 @@ def workload_kwargs(name: str, window: int = None):
     return kw
 
 
-def make_data(name: str, seed_offset: int = 0, window: int = None):
+def make_data(name: str, seed_offset: int = 0, window: int = None, templates: int = None):
     from gisspa_b200 import synth
     kw = workload_kwargs(name, window)
+    if templates:
+        kw["n_templates"] = templates
     seed = kw.pop("seed") + seed_offset
     return synth.make_dataset(seed, **kw), kw
 
@@ -215,11 +217,13 @@ def run_ours(args, rank, world, local_rank):
         import torch.distributed as dist
         dist.barrier()
     torch.cuda.set_device(local_rank)
-    ds, kw = make_data(args.workload, seed_offset=rank)
+    ds, kw = make_data(args.workload, seed_offset=rank, templates=args.templates)
     m = ds.micrographs[0]
     ny, nx = m.image.shape
     ctf = (m.defocus, m.dfdiff, m.dfang)
     params = params_for(ds, kw)
+    if args.phistep:
+        params.phi_step = args.phistep
     ctx = G.Context(local_rank)
     t0 = time.perf_counter()
     ctx.set_templates(params, ds.templates, ctf)
@@ -308,6 +312,7 @@ def run_ours(args, rank, world, local_rank):
                                      "window 512 overlap 128"),
                    "nx": nx, "ny": ny, "templates": nt, "angles": na, "windows": nw, "l": l,
                    "units_per_micrograph": na * nw * nt,
+                   "reduced_for_profiling": bool(args.templates or args.phistep),
                    "parallelism": "replicas x%d" % world,
                    "l2": "inputs larger than L2 (template set %.1f GB, pair spectra %.1f GB per angle)"
                          % (nt * l2 * 4 / 1e9, npairs * l2 * 8 / 1e9)},
@@ -410,6 +415,9 @@ def main() -> int:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["full", "small"], default="full")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    # profiling aids (smaller captures); a line produced with them names the reduced workload
+    ap.add_argument("--templates", type=int, default=None, help="use only the first N templates")
+    ap.add_argument("--phistep", type=float, default=None, help="override the in-plane angle step")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
