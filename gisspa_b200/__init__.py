@@ -69,7 +69,8 @@ PICK_DTYPE = np.dtype([("angle_index", "<i4"), ("phi", "<f4"), ("window_x", "<i4
 EXPORTS = ("gs_status_string", "gs_version", "gs_params_default", "gs_ctx_create",
            "gs_ctx_destroy", "gs_ctx_last_error", "gs_set_templates", "gs_get_geometry",
            "gs_search", "gs_search_device", "gs_get_units", "gs_picks_free", "gs_get_timings",
-           "gs_get_stats", "gs_set_kernel_timing", "gs_set_option")
+           "gs_get_stats", "gs_set_kernel_timing", "gs_set_option",
+           "gs_correlate_window_noalloc")
 
 _lib_handle = None
 
@@ -111,6 +112,8 @@ def load_library(path: Optional[str] = None) -> C.CDLL:
     lib.gs_get_timings.argtypes = [vp, C.POINTER(C.c_float), C.c_int]
     lib.gs_set_kernel_timing.argtypes = [vp, C.c_int]
     lib.gs_set_option.argtypes = [vp, C.c_int, C.c_int]
+    lib.gs_correlate_window_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                                C.c_float, C.c_void_p, C.c_void_p]
     lib.gs_get_stats.argtypes = [vp, C.POINTER(GsStats)]
     if path is None:
         _lib_handle = lib
@@ -244,6 +247,22 @@ class Context:
     def set_kernel_timing(self, enable: bool) -> None:
         self._check(self._lib.gs_set_kernel_timing(self._h, 1 if enable else 0),
                     "gs_set_kernel_timing")
+
+
+NOALLOC_SCRATCH_BYTES = 32 << 20
+NOALLOC_MAX_WINDOW = 2012
+
+
+def correlate_window_noalloc(d_window_spectrum: int, d_pair_spectra: int, n_templates: int,
+                             l: int, d_m: float, d_units: int, stream: int = 0) -> None:
+    """gs_correlate_window_noalloc on raw device pointers (no device
+    allocation; work queued on ``stream``, the call does not wait)."""
+    lib = load_library()
+    st = lib.gs_correlate_window_noalloc(C.c_void_p(d_window_spectrum), C.c_void_p(d_pair_spectra),
+                                         int(n_templates), int(l), float(d_m),
+                                         C.c_void_p(d_units), C.c_void_p(stream or None))
+    if st != GS_OK:
+        raise GisspaError(st, "gs_correlate_window_noalloc(l=%d, n_templates=%d)" % (l, n_templates))
 
 
 def run_config(config_path: str, device: Optional[int] = None, return_units: bool = False):

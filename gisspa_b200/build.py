@@ -47,7 +47,8 @@ def build_library(force: bool = False) -> str:
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
     _run([NVCC] + NVCC_FLAGS + ARCH + ["-shared", "-I" + INCLUDE, "-o", LIB,
-                                       os.path.join(CSRC, "gisspa.cu")])
+                                       os.path.join(CSRC, "gisspa.cu"),
+                                       os.path.join(CSRC, "noalloc.cu")])
     return LIB
 
 

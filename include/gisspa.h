@@ -178,6 +178,33 @@ typedef struct gs_stats {
 } gs_stats;
 int gs_get_stats(struct gs_ctx* ctx, gs_stats* out);
 
+/* Correlation of one window with a set of templates, allocating nothing.
+ * This entry point has no counterpart in the reference; it serves callers
+ * that may not allocate device memory while they run (code being captured
+ * into a CUDA graph, allocator-free real-time sections, hosts that hand the
+ * library fixed buffers and forbid it to grow).  The caller passes device
+ * buffers:
+ *   d_window_spectrum  l x l complex (interleaved re, im float32): the window
+ *                      spectrum as the search builds it (FFT / l^2, scaled);
+ *   d_pair_spectra     ceil(n_templates/2) x l x l complex: for templates
+ *                      2p and 2p+1, P_p = T_2p - i T_2p+1, T_j the spectrum
+ *                      of normalised, rotated, masked template j (FFT / l^2);
+ *   d_units            n_templates results (score, pos, peak, sigma) for
+ *                      this window, as gs_get_units reports them.
+ * The intermediate maps, accumulators and twiddles live in one static device
+ * array of GS_NOALLOC_SCRATCH_BYTES that every GPU loading this library holds
+ * until process exit; l is limited to GS_NOALLOC_MAX_WINDOW (larger windows,
+ * odd l, or l with too many prime factors return GS_ERR_UNSUPPORTED).
+ * Work is queued on `stream` (a cudaStream_t, NULL = default stream) and the
+ * call returns without waiting.  The first call on a device looks up the
+ * array's device address and must come before any stream capture.  All calls
+ * share the array and it keeps the last call's contents: calls that overlap
+ * on the GPU (other streams, other host threads) race. */
+#define GS_NOALLOC_SCRATCH_BYTES (32u << 20)
+#define GS_NOALLOC_MAX_WINDOW 2012
+int gs_correlate_window_noalloc(const float* d_window_spectrum, const float* d_pair_spectra,
+                                int n_templates, int l, float d_m, gs_unit* d_units, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
