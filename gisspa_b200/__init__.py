@@ -244,6 +244,29 @@ class Context:
         """Force the generic mixed-radix kernels (cross-check of the fast path)."""
         self._check(self._lib.gs_set_option(self._h, 1, 1 if enable else 0), "gs_set_option")
 
+    def set_two_pass(self, enable: bool) -> None:
+        """Run the correlation as per-window row and column launches instead of
+        one persistent launch per angle (cross-check of the persistent kernel)."""
+        self._check(self._lib.gs_set_option(self._h, 2, 1 if enable else 0), "gs_set_option")
+
+    def set_window_block(self, windows: int) -> None:
+        """Windows per block of the persistent kernel's unit order."""
+        self._check(self._lib.gs_set_option(self._h, 3, int(windows)), "gs_set_option")
+
+    def set_corr_ring(self, slots: int, lag: int) -> None:
+        """Scratch-map ring size and column-tile lag of the persistent kernel."""
+        # order matters: each call checks slots > lag against the current other value
+        if slots > self._lag_now():
+            self._check(self._lib.gs_set_option(self._h, 4, int(slots)), "gs_set_option")
+            self._check(self._lib.gs_set_option(self._h, 5, int(lag)), "gs_set_option")
+        else:
+            self._check(self._lib.gs_set_option(self._h, 5, int(lag)), "gs_set_option")
+            self._check(self._lib.gs_set_option(self._h, 4, int(slots)), "gs_set_option")
+        self._lag = int(lag)
+
+    def _lag_now(self) -> int:
+        return getattr(self, "_lag", 6)
+
     def set_kernel_timing(self, enable: bool) -> None:
         self._check(self._lib.gs_set_kernel_timing(self._h, 1 if enable else 0),
                     "gs_set_kernel_timing")

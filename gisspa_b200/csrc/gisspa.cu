@@ -6,6 +6,7 @@
 // micrograph preprocessing, window spectra, then for every in-plane angle the
 // template-pair spectra and, for every window, the fused correlation passes.
 #include "gisspa.h"
+#include "corr.cuh"
 #include "fastfft.cuh"
 #include "kernels.cuh"
 
@@ -55,6 +56,10 @@ struct gs_ctx {
     float timings[GS_TIMING_COUNT] = {0, 0, 0, 0, 0, 0, 0, 0};
     bool kernel_timing = false;
     bool generic_fft = false;
+    bool two_pass = false;
+    int window_block = 4;
+    int corr_slots = 16, corr_lag = 6;
+    DBuf unit_wp, dep_counters, pacc, flags;
     std::vector<cudaEvent_t> kev;  // pool of events for per-kernel timing
     gs_stats counters{0, 0, 0};
 };
@@ -209,6 +214,32 @@ int run_fast(gs_ctx* ctx, int l, int nimg, IO io) {
     }
 }
 
+template <int N2>
+int launch_corr_n2(gs_ctx* ctx, const CorrArgs& a, long long total_items) {
+    const size_t smem = CorrSmem<N2>::bytes;
+    auto kern = k_corr_persistent<N2>;
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0, nsm = 0, dev = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
+    if (per_sm < 1) return set_err(ctx, GS_ERR_UNSUPPORTED, "persistent kernel does not fit on an SM");
+    const long long grid = std::min<long long>((long long)nsm * per_sm, total_items);
+    kern<<<(unsigned)grid, 256, smem, ctx->stream>>>(a);
+    ++ctx->counters.kernel_launches;
+    CKL();
+    return GS_OK;
+}
+
+int launch_corr(gs_ctx* ctx, int l, const CorrArgs& a, long long total_items) {
+    switch (l / 16) {
+        case 32: return launch_corr_n2<32>(ctx, a, total_items);
+        case 45: return launch_corr_n2<45>(ctx, a, total_items);
+        case 48: return launch_corr_n2<48>(ctx, a, total_items);
+        default: return set_err(ctx, GS_ERR_UNSUPPORTED, "no persistent kernel for %d", l);
+    }
+}
+
 // Row / column geometry of a batch of row-major h x w images (vectors of
 // length w for rows, h for columns).
 VecGeom rows_of(int w, int h) { return VecGeom{h, (long long)w, 1, (long long)w * h}; }
@@ -340,7 +371,8 @@ int gs_ctx_destroy(gs_ctx* ctx) {
     for (auto& kv : ctx->plans) cudaFree(kv.second.tw);
     DBuf* bufs[] = {&ctx->tmpl, &ctx->in, &ctx->q, &ctx->cimg, &ctx->img, &ctx->stats, &ctx->ra, &ctx->rb,
                     &ctx->off, &ctx->win, &ctx->wsum, &ctx->winv, &ctx->tspec, &ctx->scratch, &ctx->pstats,
-                    &ctx->coef, &ctx->acc, &ctx->units, &ctx->picks, &ctx->count};
+                    &ctx->coef, &ctx->acc, &ctx->units, &ctx->picks, &ctx->count, &ctx->unit_wp,
+                    &ctx->dep_counters, &ctx->pacc, &ctx->flags};
     for (DBuf* b : bufs) free_buf(*b);
     for (cudaEvent_t e : ctx->kev) cudaEventDestroy(e);
     cudaStreamDestroy(ctx->stream);
@@ -496,7 +528,7 @@ static int search_impl(gs_ctx* ctx, const float* d_mic, int nx, int ny, const gs
     float* q2 = q1 + npix;
     k_mic_quot<<<blocks_for(npix, 256), 256, 0, ctx->stream>>>(d_mic, npix, nx, ny, q1, q2);
     ++ctx->counters.kernel_launches;
-    k_mic_seq<<<1, 32, 0, ctx->stream>>>(q1, q2, npix, P<MicStats>(ctx->stats));
+    k_mic_seq<<<1, 1024, 0, ctx->stream>>>(q1, q2, npix, P<MicStats>(ctx->stats));
     ++ctx->counters.kernel_launches;
     k_mic_clamp<<<blocks_for(npix, 256), 256, 0, ctx->stream>>>(d_mic, npix, P<MicStats>(ctx->stats), p.invert,
                                                                  P<float2>(ctx->cimg));
@@ -574,11 +606,29 @@ static int search_impl(gs_ctx* ctx, const float* d_mic, int nx, int ny, const gs
 
     // ---- angle loop (main.cu:1232-1257) ----
     TRY(ensure(ctx, ctx->tspec, sizeof(float2) * l2 * Np));
-    TRY(ensure(ctx, ctx->scratch, sizeof(float2) * l2 * Np));
+    TRY(ensure(ctx, ctx->scratch, sizeof(float2) * l2 * (fast_ok(ctx, l) && !ctx->two_pass ? ctx->corr_slots : Np)));
     TRY(ensure(ctx, ctx->pstats, sizeof(double) * 2 * N));
     TRY(ensure(ctx, ctx->coef, sizeof(float4) * Np));
     TRY(ensure(ctx, ctx->acc, sizeof(UnitAcc) * N));
     TRY(ensure(ctx, ctx->units, sizeof(UnitOut) * std::max<long long>(1, total_units)));
+    const bool persistent = fast_ok(ctx, l) && !ctx->two_pass;
+    const int nu = Np * nw;
+    const int corr_slots = ctx->corr_slots, corr_lag = ctx->corr_lag;
+    if (persistent) {
+        // unit order: blocks of window_block windows; inside a block, pair-major
+        std::vector<int2> wp;
+        wp.reserve(nu);
+        const int wbk = std::max(1, ctx->window_block);
+        for (int w0 = 0; w0 < nw; w0 += wbk)
+            for (int pp = 0; pp < Np; ++pp)
+                for (int w = w0; w < std::min(nw, w0 + wbk); ++w) wp.push_back(make_int2(w, pp));
+        TRY(ensure(ctx, ctx->unit_wp, sizeof(int2) * nu));
+        CK(cudaMemcpyAsync(ctx->unit_wp.p, wp.data(), sizeof(int2) * nu, cudaMemcpyHostToDevice, ctx->stream));
+        TRY(ensure(ctx, ctx->dep_counters, sizeof(int) * (2 * (size_t)nu + 4)));
+        TRY(ensure(ctx, ctx->pacc, sizeof(UnitAcc) * 2 * (size_t)nu));
+        TRY(ensure(ctx, ctx->flags, sizeof(int) * 4));
+        CK(cudaMemsetAsync(ctx->flags.p, 0, sizeof(int) * 4, ctx->stream));
+    }
     float2* TS = P<float2>(ctx->tspec);
     float2* R = P<float2>(ctx->scratch);
     UnitAcc* acc = P<UnitAcc>(ctx->acc);
@@ -624,7 +674,33 @@ static int search_impl(gs_ctx* ctx, const float* d_mic, int nx, int ny, const gs
             TRY(run_fft<false>(ctx, l, cols_of(l, l), Np, IoComplex{TS, (float)(1.0 / (double)l2)}));
         }
         CK(cudaEventRecord(eb, ctx->stream));
-        for (int w = 0; w < nw; ++w) {
+        if (persistent) {
+            int* cnt = P<int>(ctx->dep_counters);
+            CK(cudaMemsetAsync(cnt, 0, sizeof(int) * (2 * (size_t)nu + 4), ctx->stream));
+            CK(cudaMemsetAsync(ctx->pacc.p, 0, sizeof(UnitAcc) * 2 * (size_t)nu, ctx->stream));
+            CorrArgs ca;
+            ca.W = W; ca.P = TS; ca.R = R;
+            ca.unit_wp = P<int2>(ctx->unit_wp);
+            ca.done_rows = cnt; ca.done_cols = cnt + nu;
+            ca.acc = P<UnitAcc>(ctx->pacc);
+            ca.out = units + (size_t)ai * nw * N;
+            ca.next_item = cnt + 2 * (size_t)nu;
+            ca.error = P<int>(ctx->flags);
+            ca.nu = nu; ca.ntmpl = N; ca.S = corr_slots; ca.lag = corr_lag; ca.L2 = l2;
+            // border interval of unshifted indices: X = (x + l/2) mod l is masked
+            // when X < d_m/4 or X > l - d_m/4 (GPU_func.cu:681)
+            {
+                const int h = l / 2;
+                int ya = (int)ceilf(q_lo), yb = (int)floorf(q_hi);
+                ca.yb0 = yb - h + 1;
+                ca.yb1 = ya + h - 1;
+                if (ca.yb1 < ca.yb0) { ca.yb0 = 1; ca.yb1 = 0; }
+            }
+            if (ctx->kernel_timing) CK(cudaEventRecord(ctx->kev[0], ctx->stream));
+            TRY(launch_corr(ctx, l, ca, (long long)(nu + corr_lag) * 2 * (l / 16)));
+            if (ctx->kernel_timing) CK(cudaEventRecord(ctx->kev[1], ctx->stream));
+        }
+        for (int w = 0; w < nw && !persistent; ++w) {
             CK(cudaMemsetAsync(acc, 0, sizeof(UnitAcc) * N, ctx->stream));
             const bool fast = fast_ok(ctx, l);
             if (ctx->kernel_timing) CK(cudaEventRecord(ctx->kev[4 * w + 0], ctx->stream));
@@ -655,7 +731,12 @@ static int search_impl(gs_ctx* ctx, const float* d_mic, int nx, int ny, const gs
         cudaEventElapsedTime(&t2, eb, ec);
         ms_spec += t1;
         ms_corr += t2;
-        if (ctx->kernel_timing) {
+        if (ctx->kernel_timing && persistent) {
+            float a = 0;
+            cudaEventElapsedTime(&a, ctx->kev[0], ctx->kev[1]);
+            k1ms += a;
+            k1n += 1;
+        } else if (ctx->kernel_timing) {
             for (int w = 0; w < nw; ++w) {
                 float a = 0, b = 0;
                 cudaEventElapsedTime(&a, ctx->kev[4 * w + 0], ctx->kev[4 * w + 1]);
@@ -666,6 +747,12 @@ static int search_impl(gs_ctx* ctx, const float* d_mic, int nx, int ny, const gs
             k1n += nw;
             k2n += nw;
         }
+    }
+    if (persistent) {
+        int flag = 0;
+        CK(cudaMemcpyAsync(&flag, ctx->flags.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (flag) return set_err(ctx, GS_ERR_TIMEOUT, "correlation kernel: a bounded dependency wait gave up");
     }
     ctx->last_na = na;
     ctx->last_nw = nw;
@@ -785,6 +872,19 @@ int gs_set_option(gs_ctx* ctx, int option, int value) {
     if (!ctx) return GS_ERR_ARG;
     switch (option) {
         case GS_OPT_GENERIC_FFT: ctx->generic_fft = value != 0; return GS_OK;
+        case GS_OPT_TWO_PASS: ctx->two_pass = value != 0; return GS_OK;
+        case GS_OPT_CORR_SLOTS:
+            if (value <= ctx->corr_lag) return set_err(ctx, GS_ERR_ARG, "slots must exceed the lag");
+            ctx->corr_slots = value;
+            return GS_OK;
+        case GS_OPT_CORR_LAG:
+            if (value < 0 || value >= ctx->corr_slots) return set_err(ctx, GS_ERR_ARG, "lag must be in [0, slots)");
+            ctx->corr_lag = value;
+            return GS_OK;
+        case GS_OPT_WINDOW_BLOCK:
+            if (value < 1) return set_err(ctx, GS_ERR_ARG, "window block must be >= 1");
+            ctx->window_block = value;
+            return GS_OK;
         default: return set_err(ctx, GS_ERR_ARG, "unknown option %d", option);
     }
 }

@@ -186,23 +186,53 @@ __global__ void k_mic_quot(const float* __restrict__ img, long long n, int nx, i
 
 // The two float32 running sums of main.cu:530-535 in their exact sequential
 // order (float addition is not associative, and the reference's clamp bounds
-// are integers cut from these sums, main.cu:536-543).  One warp: lanes load
-// 32 consecutive terms, every lane adds them in order from shuffles.
-__global__ void k_mic_seq(const float* __restrict__ q1, const float* __restrict__ q2, long long n,
-                          MicStats* __restrict__ out) {
-    const int lane = threadIdx.x & 31;
+// are integers cut from these sums, main.cu:536-543).  One CTA: thread 0 adds
+// the terms in order from a shared-memory chunk while warps 1.. stage the
+// next chunk (double buffer); the two sums are independent chains, so the
+// loop runs at about one add latency per term.
+constexpr int kSeqChunk = 2048;
+__global__ void __launch_bounds__(1024) k_mic_seq(const float* __restrict__ q1, const float* __restrict__ q2,
+                                                  long long n, MicStats* __restrict__ out) {
+    __shared__ __align__(16) float b1[2][kSeqChunk];
+    __shared__ __align__(16) float b2[2][kSeqChunk];
+    const int tid = threadIdx.x;
     float s1 = 0.0f, s2 = 0.0f;
-    for (long long base = 0; base < n; base += 32) {
-        const long long idx = base + lane;
-        const float a = idx < n ? q1[idx] : 0.0f;
-        const float b = idx < n ? q2[idx] : 0.0f;
-        const int cnt = (int)min((long long)32, n - base);
-        for (int j = 0; j < cnt; ++j) {
-            s1 = __fadd_rn(s1, __shfl_sync(0xffffffffu, a, j));
-            s2 = __fadd_rn(s2, __shfl_sync(0xffffffffu, b, j));
-        }
+    // stage chunk 0
+    for (int i = tid; i < kSeqChunk; i += blockDim.x) {
+        const long long g = i;
+        b1[0][i] = g < n ? q1[g] : 0.0f;
+        b2[0][i] = g < n ? q2[g] : 0.0f;
     }
-    if (lane == 0) {
+    int buf = 0;
+    for (long long base = 0; base < n; base += kSeqChunk) {
+        __syncthreads();  // chunk `buf` is staged; chunk buf^1 is free
+        if (tid == 0) {
+            const int cnt = (int)min((long long)kSeqChunk, n - base);
+            const float4* v1 = reinterpret_cast<const float4*>(b1[buf]);
+            const float4* v2 = reinterpret_cast<const float4*>(b2[buf]);
+            int i = 0;
+            for (; i + 4 <= cnt; i += 4) {
+                const float4 a = v1[i >> 2], c = v2[i >> 2];
+                s1 = __fadd_rn(s1, a.x); s2 = __fadd_rn(s2, c.x);
+                s1 = __fadd_rn(s1, a.y); s2 = __fadd_rn(s2, c.y);
+                s1 = __fadd_rn(s1, a.z); s2 = __fadd_rn(s2, c.z);
+                s1 = __fadd_rn(s1, a.w); s2 = __fadd_rn(s2, c.w);
+            }
+            for (; i < cnt; ++i) {
+                s1 = __fadd_rn(s1, b1[buf][i]);
+                s2 = __fadd_rn(s2, b2[buf][i]);
+            }
+        } else if (tid >= 32) {
+            const long long nb = base + kSeqChunk;
+            for (int i = tid - 32; i < kSeqChunk; i += blockDim.x - 32) {
+                const long long g = nb + i;
+                b1[buf ^ 1][i] = g < n ? q1[g] : 0.0f;
+                b2[buf ^ 1][i] = g < n ? q2[g] : 0.0f;
+            }
+        }
+        buf ^= 1;
+    }
+    if (tid == 0) {
         const float avg = s1;
         const float aa = __fmul_rn(avg, avg);
         const float var = __fsqrt_rn(__fsub_rn(s2, aa));

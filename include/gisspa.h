@@ -155,7 +155,9 @@ void gs_picks_free(gs_pick* picks);
  *  [2] correlation ms (all angles)    [3] total ms
  *  [4] row-pass kernel ms (sum)       [5] row-pass launches
  *  [6] column-pass kernel ms (sum)    [7] column-pass launches
- * Entries 4-7 are filled only while per-kernel timing is enabled. */
+ * With the persistent correlation kernel, [4]/[5] hold its time and launches
+ * and [6]/[7] are zero.  Entries 4-7 are filled only while per-kernel timing
+ * is enabled. */
 #define GS_TIMING_COUNT 8
 int gs_get_timings(struct gs_ctx* ctx, float* out, int n);
 
@@ -167,6 +169,18 @@ int gs_set_kernel_timing(struct gs_ctx* ctx, int enable);
  * GS_OPT_GENERIC_FFT: 1 = always use the generic mixed-radix kernels, 0 =
  * use the specialised l = 16*N2 kernels where they exist (default). */
 #define GS_OPT_GENERIC_FFT 1
+/* GS_OPT_TWO_PASS: 1 = run the correlation as separate row and column
+ * launches per window, 0 = one persistent launch per angle where the
+ * specialised kernels exist (default). */
+#define GS_OPT_TWO_PASS 2
+/* GS_OPT_WINDOW_BLOCK: windows per block of the persistent launch's unit
+ * order (reuse of window and pair spectra in L2); default 4. */
+#define GS_OPT_WINDOW_BLOCK 3
+/* GS_OPT_CORR_SLOTS / GS_OPT_CORR_LAG: scratch maps in the persistent
+ * launch's ring (default 16) and how many units after its row tiles a unit's
+ * column tiles are queued (default 6); slots must exceed lag. */
+#define GS_OPT_CORR_SLOTS 4
+#define GS_OPT_CORR_LAG 5
 int gs_set_option(struct gs_ctx* ctx, int option, int value);
 
 /* Counters of this context since creation (no reference counterpart; the

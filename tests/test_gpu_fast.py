@@ -87,3 +87,31 @@ def test_fast_sizes_match_oracle(l, overlap):
     assert rel.max() <= H.SCORE_RTOL, rel.max()
     assert np.array_equal(u["pos"][fin], ref.pos[fin])
     assert len(picks) == len(ref.picks)
+
+
+def test_persistent_equals_two_pass(tmp_path):
+    """One persistent launch per angle (dependency-tracked row/column tiles,
+    scratch ring) against per-window row and column launches, and against
+    other unit orders (window blocks of 1 and 5)."""
+    H.materialize("bench_small", str(tmp_path))
+    cfg = formats.read_config(str(tmp_path / "config"))
+    ent = formats.read_lst_entry(str(tmp_path / cfg.inlst), 0)
+    img = formats.read_mrc(ent.path, 0)
+    stack = formats.read_mrc(str(tmp_path / cfg.temp2d), -1)
+    ctf = (ent.defocus, ent.dfdiff, ent.dfang)
+    tabs = []
+    for two_pass, block in ((True, 4), (False, 4), (False, 1), (False, 5)):
+        with G.Context(0) as ctx:
+            ctx.set_two_pass(two_pass)
+            ctx.set_window_block(block)
+            ctx.set_templates(G.params_from_config(cfg), stack, ctf)
+            picks = ctx.search(img, ctf)
+            tabs.append((ctx.units(), picks))
+    ref, ref_picks = tabs[0]
+    fin = np.isfinite(ref["score"])
+    for u, picks in tabs[1:]:
+        assert np.array_equal(fin, np.isfinite(u["score"]))
+        rel = np.abs(u["score"][fin] - ref["score"][fin]) / np.abs(ref["score"][fin])
+        assert rel.max() < 1e-6, rel.max()
+        assert np.array_equal(u["pos"], ref["pos"])
+        assert len(picks) == len(ref_picks)
