@@ -12,18 +12,24 @@
 //
 // Dependencies and why they cannot deadlock: a column tile of u waits until
 // all N2 row tiles of u are done; a row tile of u >= S waits until all
-// column tiles of u - S are done (its scratch slot is free).  Both wait only
+// column tiles of u - S are done (its scratch slot is free).  Completion is
+// counted per warp (every warp of a tile fences its own stores or atomics and
+// increments the unit's counter), so a unit is done at 8 N2 increments and no
+// CTA-wide barrier is needed to publish a tile.  Both wait only
 // on items that come earlier in the claim order, and an item is claimed only
 // by a running CTA that finishes it before claiming another, so the earliest
 // unfinished item can always proceed.  Every wait is bounded; a wait that
 // gives up raises the error flag (reported as GS_ERR_TIMEOUT) and the item
 // still completes and signals, so no other CTA is left waiting on it.
 //
-// Memory ordering: producers store the maps with st.global.cg, then
-// __syncthreads(), and one thread issues __threadfence() + atomicAdd on the
-// unit's counter; consumers spin with ld.acquire.gpu, __syncthreads(), and
-// read the maps with ld.global.cg (L2, never a stale L1 line from an earlier
-// occupant of the slot).
+// Memory ordering: producers store the maps bypassing L1 (st.global with an
+// L2 cache hint), then
+// __syncwarp(), and lane 0 of each warp issues __threadfence() + atomicAdd on
+// the unit's counter; the consumer CTA's thread 0 spins with ld.acquire.gpu
+// and fences before the CTA barrier that publishes the item, and its threads
+// read the maps with L1::no_allocate loads (L2, never a stale L1 line from an
+// earlier occupant of the slot).  Each item costs two CTA barriers: step 1 -> step 2
+// of the FFT, and the end-of-item barrier that hands over the next item.
 #pragma once
 
 #include "fastfft.cuh"
@@ -53,7 +59,8 @@ __device__ __forceinline__ int ld_acquire_gpu(const int* p) {
 }
 
 // Thread 0 waits until *p >= target; bounded (about a second or more), then
-// flags the error and gives up.  Must be followed by __syncthreads().
+// flags the error and gives up.  A CTA barrier must follow before other
+// threads rely on the condition.
 __device__ __forceinline__ void wait_counter(const int* p, int target, int* error) {
     if (threadIdx.x != 0) return;
     if (ld_acquire_gpu(p) >= target) return;
@@ -67,14 +74,41 @@ __device__ __forceinline__ void wait_counter(const int* p, int target, int* erro
     atomicExch(error, 1);
 }
 
+constexpr int kCorrWarps = 8;  // warps per CTA (256 threads)
+
 template <int N2>
 struct CorrSmem {
     using F = Fast16<N2>;
     static constexpr size_t tile = (size_t)F::V * F::VP * sizeof(float2);
     static constexpr size_t tw = (size_t)16 * N2 * sizeof(float2);
     static constexpr size_t red = 128 * sizeof(double);
-    static constexpr size_t bytes = tile + tw + red + 16;
+    static constexpr size_t bytes = tile + tw + red + 32;
 };
+
+// L2 eviction-priority hints: scratch maps are stored "evict last" (they are
+// read again shortly) and loaded "evict first" by their only reader; the
+// window spectra, reused by every pair of a window block, are loaded
+// "evict last".
+__device__ __forceinline__ unsigned long long l2_policy_evict_last() {
+    unsigned long long p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ unsigned long long l2_policy_evict_first() {
+    unsigned long long p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ float2 ld_l2hint(const float2* ptr, unsigned long long pol) {
+    float2 v;
+    asm volatile("ld.global.L1::no_allocate.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;"
+                 : "=f"(v.x), "=f"(v.y) : "l"(ptr), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ void st_l2hint(float2* ptr, float2 v, unsigned long long pol) {
+    asm volatile("st.global.L1::no_allocate.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;"
+                 :: "l"(ptr), "f"(v.x), "f"(v.y), "l"(pol) : "memory");
+}
 
 template <int N2>
 __device__ __forceinline__ void corr_row_tile(const CorrArgs& a, int u, int t, float2* tile, const float2* twt) {
@@ -85,12 +119,14 @@ __device__ __forceinline__ void corr_row_tile(const CorrArgs& a, int u, int t, f
     const float2* Pr = a.P + (long long)wp.y * a.L2;
     float2* Rs = a.R + (long long)(u % a.S) * a.L2;
     const int r0 = t * F::V;
+    const unsigned long long keep = l2_policy_evict_last();
     for (int task = threadIdx.x; task < F::V * N2; task += F::kThreads) {
         const int v = task / N2, n2 = task - v * N2;
         const long long base = (long long)(r0 + v) * L + n2;
         float2 x[16];
 #pragma unroll
-        for (int n1 = 0; n1 < 16; ++n1) x[n1] = cmulc(__ldg(Wr + base + N2 * n1), __ldg(Pr + base + N2 * n1));
+        for (int n1 = 0; n1 < 16; ++n1)
+            x[n1] = cmulc(ld_l2hint(Wr + base + N2 * n1, keep), __ldg(Pr + base + N2 * n1));
         rf::rfft<16, 1, true>(x);
         float2* dst = tile + v * F::VP + n2;
         const float2* tw = twt + n2;
@@ -111,25 +147,32 @@ __device__ __forceinline__ void corr_row_tile(const CorrArgs& a, int u, int t, f
         float2* dst = Rs + (long long)(r0 + v) * L + k1;
         rf::static_for<N2>([&](auto kc) {
             constexpr int k2 = decltype(kc)::value;
-            __stcg(dst + 16 * k2, b[rf::rpos<N2>(k2)]);
+            st_l2hint(dst + 16 * k2, b[rf::rpos<N2>(k2)], keep);
         });
+    }
+    // publish this warp's share of the tile
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) {
+        __threadfence();
+        atomicAdd(&a.done_rows[u], 1);
     }
 }
 
 template <int N2>
 __device__ __forceinline__ void corr_col_tile(const CorrArgs& a, int u, int t, float2* tile, const float2* twt,
-                                              double* red, bool* last_out) {
+                                              bool* last_out) {
     using F = Fast16<N2>;
     constexpr int L = F::L;
     constexpr int h = L / 2;
     const float2* Rs = a.R + (long long)(u % a.S) * a.L2;
     const int c0 = t * F::V;
+    const unsigned long long drop = l2_policy_evict_first();
     for (int task = threadIdx.x; task < F::V * N2; task += F::kThreads) {
         const int n2 = task / F::V, v = task - n2 * F::V;
         const float2* src = Rs + (long long)n2 * L + c0 + v;
         float2 x[16];
 #pragma unroll
-        for (int n1 = 0; n1 < 16; ++n1) x[n1] = __ldcg(src + (long long)N2 * n1 * L);
+        for (int n1 = 0; n1 < 16; ++n1) x[n1] = ld_l2hint(src + (long long)N2 * n1 * L, drop);
         rf::rfft<16, 1, true>(x);
         float2* dst = tile + v * F::VP + n2;
         const float2* tw = twt + n2;
@@ -181,29 +224,24 @@ __device__ __forceinline__ void corr_col_tile(const CorrArgs& a, int u, int t, f
         const int Y = y + h < L ? y + h : y - h;
         kb = argmax_key(best2, Y * L + X);
     }
-    double s[4] = {s1a, s2a, s1b, s2b};
+    // warp-level reduction, then one set of atomics per warp (no CTA barrier)
+    double d1a = warp_sum((double)s1a), d2a = warp_sum((double)s2a);
+    double d1b = warp_sum((double)s1b), d2b = warp_sum((double)s2b);
     ka = warp_max_u64(ka);
     kb = warp_max_u64(kb);
-    block_sum<4>(s, red);
-    unsigned long long* ks = reinterpret_cast<unsigned long long*>(red);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) { ks[warp] = ka; ks[32 + warp] = kb; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        for (int w2 = 0; w2 < F::kThreads / 32; ++w2) {
-            ka = ks[w2] > ka ? ks[w2] : ka;
-            kb = ks[32 + w2] > kb ? ks[32 + w2] : kb;
-        }
+    bool last = false;
+    if ((threadIdx.x & 31) == 0) {
         UnitAcc* ac = a.acc + 2 * (long long)u;
         if (ka) atomicMax(&ac[0].key, ka);
-        atomicAdd(&ac[0].s1, s[0]);
-        atomicAdd(&ac[0].s2, s[1]);
+        atomicAdd(&ac[0].s1, d1a);
+        atomicAdd(&ac[0].s2, d2a);
         if (kb) atomicMax(&ac[1].key, kb);
-        atomicAdd(&ac[1].s1, s[2]);
-        atomicAdd(&ac[1].s2, s[3]);
+        atomicAdd(&ac[1].s1, d1b);
+        atomicAdd(&ac[1].s2, d2b);
         __threadfence();
-        *last_out = atomicAdd(&a.done_cols[u], 1) == N2 - 1;
+        last = atomicAdd(&a.done_cols[u], 1) == kCorrWarps * N2 - 1;
     }
+    *last_out = last;  // meaningful in lane 0 only
 }
 
 // Score of one template from its accumulators (main.cu:869-876).
@@ -221,6 +259,19 @@ __device__ __forceinline__ UnitOut unit_score(const UnitAcc& ac, int l) {
     return u;
 }
 
+// Thread 0 claims and resolves the dependency of the next item while the
+// CTA works on the current one; one barrier publishes it.
+template <int N2>
+__device__ __forceinline__ void corr_wait_for(const CorrArgs& a, int item) {
+    const int s = item / (2 * N2), j = item - s * (2 * N2);
+    if (j < N2) {
+        if (s < a.nu && s >= a.S) wait_counter(a.done_cols + (s - a.S), kCorrWarps * N2, a.error);
+    } else {
+        const int u = s - a.lag;
+        if (u >= 0 && u < a.nu) wait_counter(a.done_rows + u, kCorrWarps * N2, a.error);
+    }
+}
+
 template <int N2>
 __global__ void __launch_bounds__(256, 2) k_corr_persistent(CorrArgs a) {
     using F = Fast16<N2>;
@@ -228,45 +279,36 @@ __global__ void __launch_bounds__(256, 2) k_corr_persistent(CorrArgs a) {
     extern __shared__ __align__(16) unsigned char smc[];
     float2* tile = reinterpret_cast<float2*>(smc);
     float2* twt = reinterpret_cast<float2*>(smc + SM::tile);
-    double* red = reinterpret_cast<double*>(smc + SM::tile + SM::tw);
-    int* ish = reinterpret_cast<int*>(smc + SM::tile + SM::tw + SM::red);
-    bool* last = reinterpret_cast<bool*>(ish + 2);
+    int* ish = reinterpret_cast<int*>(smc + SM::tile + SM::tw + SM::red);  // ring of 4 broadcast slots
     // inverse twiddles W_L^{-n2 k1} = exp(+2 pi i n2 k1 / L), table [k1][n2]
     for (int i = threadIdx.x; i < 16 * N2; i += F::kThreads) {
         const int k1 = i / N2, n2 = i - k1 * N2;
-        double s, c;
-        sincospi(2.0 * (double)((n2 * k1) % F::L) / (double)F::L, &s, &c);
-        twt[i] = make_float2((float)c, (float)s);
+        double sn, cs;
+        sincospi(2.0 * (double)((n2 * k1) % F::L) / (double)F::L, &sn, &cs);
+        twt[i] = make_float2((float)cs, (float)sn);
     }
     const int total = (a.nu + a.lag) * 2 * N2;
-    if (threadIdx.x == 0) ish[0] = atomicAdd(a.next_item, 1);
+    if (threadIdx.x == 0) {
+        const int first = atomicAdd(a.next_item, 1);
+        if (first < total) corr_wait_for<N2>(a, first);
+        ish[0] = first;
+    }
     __syncthreads();
     int item = ish[0];
-    __syncthreads();  // every thread has read ish[0] before thread 0 writes it again
-    while (item < total) {
+    for (int iter = 1; item < total; ++iter) {
         int nxt = 0;
         if (threadIdx.x == 0) nxt = atomicAdd(a.next_item, 1);  // consumed after the tile
         const int s = item / (2 * N2), j = item - s * (2 * N2);
         if (j < N2) {
-            const int u = s;
-            if (u < a.nu) {
-                if (u >= a.S) wait_counter(a.done_cols + (u - a.S), N2, a.error);
-                __syncthreads();
-                corr_row_tile<N2>(a, u, j, tile, twt);
-                __syncthreads();
-                if (threadIdx.x == 0) {
-                    __threadfence();
-                    atomicAdd(&a.done_rows[u], 1);
-                }
+            if (s < a.nu) {
+                corr_row_tile<N2>(a, s, j, tile, twt);
             }
         } else {
             const int u = s - a.lag;
             if (u >= 0 && u < a.nu) {
-                wait_counter(a.done_rows + u, N2, a.error);
-                __syncthreads();
-                corr_col_tile<N2>(a, u, j - N2, tile, twt, red, last);
-                __syncthreads();
-                if (threadIdx.x == 0 && *last) {
+                bool last = false;
+                corr_col_tile<N2>(a, u, j - N2, tile, twt, &last);
+                if ((threadIdx.x & 31) == 0 && last) {
                     __threadfence();
                     const int2 wp = a.unit_wp[u];
                     const UnitAcc* ac = a.acc + 2 * (long long)u;
@@ -282,10 +324,15 @@ __global__ void __launch_bounds__(256, 2) k_corr_persistent(CorrArgs a) {
                 }
             }
         }
-        if (threadIdx.x == 0) ish[0] = nxt;
+        if (threadIdx.x == 0) {
+            if (nxt < total) corr_wait_for<N2>(a, nxt);
+            ish[iter & 3] = nxt;
+        }
+        // one barrier: the tile buffer is free again and the next item (with its
+        // dependency satisfied) is published; slot iter & 3 is not rewritten
+        // before every thread has passed at least one more barrier
         __syncthreads();
-        item = ish[0];
-        __syncthreads();  // as above: no thread may still be reading ish[0] when it changes
+        item = ish[iter & 3];
     }
 }
 
