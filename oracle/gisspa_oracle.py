@@ -648,6 +648,89 @@ def search(micrograph: np.ndarray, templates_raw: np.ndarray, p: Params,
                         tab["score"], tab_pos, tab["peak"], tab["sd"])
 
 
+@dataclass
+class BlockPick:
+    angle_index: int
+    euler3: float
+    phi: float
+    window_i: int
+    window_j: int
+    template: int
+    block: int
+    cx: float
+    cy: float
+    score: float
+
+
+def search_norm1(micrograph: np.ndarray, templates_raw: np.ndarray, p: Params, ctf: Ctf,
+                 ctf_first: Optional[Ctf] = None, prepared: Optional[np.ndarray] = None,
+                 workers: int = 1):
+    """norm_type 1 (main.cu:1170-1229): every correlation value is z-scored
+    against the mean and standard deviation of that window pixel over all
+    templates and angles (first sweep: compute_CCG_sum / add_CCG_to_sum /
+    set_CCG_mean, main.cu:724-756, GPU_func.cu:617-646), then in a second
+    sweep each 1024-element block of the z-scored maps reports its maximum
+    and position (update_CCG + get_peak_pos, GPU_func.cu:648-662, 711-745; no
+    border mask) and a line is written when it reaches the threshold and the
+    centre lies at least d_m inside the micrograph (main.cu:800-817).
+    Returns (picks in reference order, per-window mean, per-window std)."""
+    ny, nx = micrograph.shape
+    n, ty, tx = templates_raw.shape
+    l = adjust_padding_size(p.padding_size, tx, ty)
+    if (l * l) % 1024:
+        raise ValueError("norm_type 1 needs l*l to be a multiple of 1024")
+    if ctf_first is None:
+        ctf_first = ctf
+    T = prepared if prepared is not None else prepare_templates(templates_raw, p, l, ctf_first, workers)
+    img = preprocess_micrograph(micrograph, p, ctf, workers)
+    offx = window_offsets(nx, l, p.overlap)
+    offy = window_offsets(ny, l, p.overlap)
+    bx, by = len(offx), len(offy)
+    W = window_spectra(split_windows(img, offx, offy, l), p, workers)
+    chk = checker(l)
+    angs = angle_list(p.phi_step)
+    l2 = float(l * l)
+    s1 = np.zeros((bx * by, l, l))
+    s2 = np.zeros((bx * by, l, l))
+    spectra = []
+    for e in angs:
+        TSc = np.conj(template_spectra(T, e, p.d_m, workers)) * chk[None]
+        spectra.append(TSc)
+        for w in range(bx * by):
+            cur = _ifft2_unnorm(W[w][None] * TSc, workers).real / l2
+            s1[w] += cur.sum(axis=0)
+            s2[w] += (cur * cur).sum(axis=0)
+    total = float(n * len(angs))
+    avg = s1 / total
+    with np.errstate(invalid="ignore"):
+        std = np.sqrt(s2 / total - avg * avg)
+    nblk = (l * l) // 1024
+    d_m = float(f32(p.d_m))
+    thres = f32(p.thres)
+    picks: List[BlockPick] = []
+    for ai, e in enumerate(angs):
+        for j in range(by):
+            for i in range(bx):
+                w = i + j * bx
+                cur = _ifft2_unnorm(W[w][None] * spectra[ai], workers).real / l2
+                with np.errstate(invalid="ignore", divide="ignore"):
+                    z = np.where(std[w][None] > 0, (cur - avg[w][None]) / std[w][None], 0.0)
+                zb = z.reshape(n, nblk, 1024)
+                mx = zb.max(axis=2)
+                am = zb.argmax(axis=2)
+                for J in range(n):
+                    for b in range(nblk):
+                        if f32(mx[J, b]) < thres:
+                            continue
+                        pos = b * 1024 + int(am[J, b])
+                        cx = float(offx[i] + pos % l)
+                        cy = float(offy[j] + pos // l)
+                        if cx >= d_m and cx < nx - d_m and cy >= d_m and cy < ny - d_m:
+                            picks.append(BlockPick(ai, float(e), float(printed_phi(e)), i, j, J, b,
+                                                   cx, cy, float(mx[J, b])))
+    return picks, avg, std
+
+
 def params_from_config(cfg) -> Params:
     """Params from a parsed config object with the reference's field names."""
     return Params(apix=cfg.apix, phi_step=cfg.phi_step, kk=cfg.kk, energy=cfg.energy,
@@ -683,9 +766,14 @@ def run_config(config_path: str, workers: int = 1, return_results: bool = False)
         ent = formats.read_lst_entry(cfg.inlst, m)
         img = formats.read_mrc(ent.path, ent.nn)
         ctf = make_ctf(p, ent.defocus, ent.dfdiff, ent.dfang, l)
-        res = search(img, raw, p, ctf, ctf0, prepared=T, workers=workers)
-        results.append(res)
-        for pk in res.picks:
+        if p.norm_type == 1:
+            picks, _, _ = search_norm1(img, raw, p, ctf, ctf0, prepared=T, workers=workers)
+            results.append(picks)
+        else:
+            res = search(img, raw, p, ctf, ctf0, prepared=T, workers=workers)
+            results.append(res)
+            picks = res.picks
+        for pk in picks:
             lines.append(format_pick_line(ent.nn, ent.path, ctf, float(eul[pk.template, 0]),
                                           float(eul[pk.template, 1]), pk))
     return (lines, results) if return_results else lines
