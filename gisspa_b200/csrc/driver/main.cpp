@@ -40,7 +40,7 @@ static void print_help() {
     printf("Lowres           = low resolution cut\n");
     printf("diameter         = target diameter in pixels\n");
     printf("Optional parameters:\n");
-    printf("norm_type        = CCG norm type (0 only)\n");
+    printf("norm_type        = 0: score = peak / sigma per map; 1: per-pixel z-score over all templates and angles\n");
     printf("invert           = 0 / 1, invert contrast\n");
     printf("threshold        = score threshold, only scores >= it are written\n");
     printf("output           = output list file name\n");

@@ -9,6 +9,7 @@
 #include "corr.cuh"
 #include "fastfft.cuh"
 #include "kernels.cuh"
+#include "norm1.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -308,6 +309,159 @@ unsigned blocks_for(long long n, int threads, unsigned cap = 1u << 30) {
 // ===========================================================================
 // C ABI
 // ===========================================================================
+// Template-pair spectra of one in-plane angle (rotate_template + the
+// normalisation and FFT of main.cu:1236-1249): TS[p] = FFT(t_2p - i t_2p+1) / l^2
+// with each rotated, masked template mean/variance normalised.
+static int pair_spectra(gs_ctx* ctx, float e, float2* TS) {
+    const int l = ctx->l, N = ctx->ntmpl, Np = (N + 1) / 2;
+    const long long l2 = (long long)l * l;
+    const double ang = (double)e * kPiRef / 180.0;
+    const float cose = (float)cos(ang), sine = (float)sin(ang);
+    CK(cudaMemsetAsync(ctx->pstats.p, 0, sizeof(double) * 2 * N, ctx->stream));
+    dim3 g(blocks_for(l2, 256, 32), Np);
+    k_pair_rotate<<<g, 256, 0, ctx->stream>>>(P<float>(ctx->tmpl), N, l, cose, sine, ctx->p.d_m, TS,
+                                              P<double>(ctx->pstats));
+    ++ctx->counters.kernel_launches;
+    k_pair_coef<<<blocks_for(Np, 128), 128, 0, ctx->stream>>>(P<double>(ctx->pstats), N, l, P<float4>(ctx->coef));
+    ++ctx->counters.kernel_launches;
+    CKL();
+    if (fast_ok(ctx, l)) {
+        TRY(run_fast<false, false>(ctx, l, Np, F16PairNorm{TS, P<float4>(ctx->coef), l, l2}));
+        TRY(run_fast<false, true>(ctx, l, Np, F16Complex<true>{TS, l, l2, (float)(1.0 / (double)l2)}));
+    } else {
+        TRY(run_fft<false>(ctx, l, rows_of(l, l), Np, IoPairNorm{TS, P<float4>(ctx->coef), l2}));
+        TRY(run_fft<false>(ctx, l, cols_of(l, l), Np, IoComplex{TS, (float)(1.0 / (double)l2)}));
+    }
+    return GS_OK;
+}
+
+// Row pass of the correlation of window spectrum Ww with the Np pair spectra
+// into the scratch maps R (inverse FFT along x of Ww conj(TS_p)).
+static int corr_rows(gs_ctx* ctx, const float2* Ww, const float2* TS, float2* R) {
+    const int l = ctx->l, Np = (ctx->ntmpl + 1) / 2;
+    const long long l2 = (long long)l * l;
+    if (fast_ok(ctx, l)) return run_fast<true, false>(ctx, l, Np, F16Pass1{Ww, TS, R, l, l2});
+    return run_fft<true>(ctx, l, rows_of(l, l), Np, IoPass1{Ww, TS, R, l2});
+}
+
+// Column pass of the correlation with a per-value epilogue (norm1.cuh).
+template <class Epi>
+static int corr_cols(gs_ctx* ctx, const float2* R, const Epi& epi) {
+    const int l = ctx->l, Np = (ctx->ntmpl + 1) / 2;
+    const long long l2 = (long long)l * l;
+    if (fast_ok(ctx, l)) return run_fast<true, true>(ctx, l, Np, F16Norm1<Epi>{R, epi, l, l2});
+    return run_fft<true>(ctx, l, cols_of(l, l), Np, IoNorm1<Epi>{R, epi});
+}
+
+// norm_type 1 (pickPartcles_CCG_NORM path, main.cu:1170-1229): sweep 1 sums
+// cc / l^2 and its square per window pixel over all templates and angles
+// (compute_CCG_sum, main.cu:724-749) and turns them into mean and standard
+// deviation (compute_CCG_mean); sweep 2 recomputes every map, z-scores it
+// and reports the maximum of every 1024-element block (main.cu:770-820).
+// Picks come out in the reference's order: angle, window row, window
+// column, template, block.
+static int search_norm1(gs_ctx* ctx, const float2* W, int nx, int ny, const std::vector<int>& offx,
+                        const std::vector<int>& offy, const std::vector<float>& angles, float* ms_spec,
+                        float* ms_corr, std::vector<gs_pick>* out) {
+    const int l = ctx->l, N = ctx->ntmpl;
+    const long long l2 = (long long)l * l;
+    const int bx = (int)offx.size(), nw = bx * (int)offy.size(), na = (int)angles.size();
+    const int nblk = (int)(l2 / 1024);
+    const float sgn = ((l / 2) % 2 == 0) ? 1.0f : -1.0f;
+    float2* TS = P<float2>(ctx->tspec);
+    float2* R = P<float2>(ctx->scratch);
+    TRY(ensure(ctx, ctx->pacc, sizeof(float) * 2 * l2 * nw));        // window moments
+    TRY(ensure(ctx, ctx->units, sizeof(unsigned long long) * (size_t)nw * N * nblk));  // block keys
+    TRY(ensure(ctx, ctx->picks, sizeof(BlockPickDev) * (size_t)nw * N * nblk));
+    TRY(ensure(ctx, ctx->count, sizeof(unsigned long long)));
+    float* s1 = P<float>(ctx->pacc);
+    float* s2 = s1 + l2 * nw;
+    unsigned long long* keys = P<unsigned long long>(ctx->units);
+    CK(cudaMemsetAsync(s1, 0, sizeof(float) * 2 * l2 * nw, ctx->stream));
+    cudaEvent_t ea, eb, ec;
+    CK(cudaEventCreate(&ea));
+    CK(cudaEventCreate(&eb));
+    CK(cudaEventCreate(&ec));
+    struct EvGuard3 { cudaEvent_t a, b, c; ~EvGuard3() { cudaEventDestroy(a); cudaEventDestroy(b); cudaEventDestroy(c); } } eg3{ea, eb, ec};
+    auto elapsed = [&](void) -> int {
+        CK(cudaEventSynchronize(ec));
+        float t1 = 0, t2 = 0;
+        cudaEventElapsedTime(&t1, ea, eb);
+        cudaEventElapsedTime(&t2, eb, ec);
+        *ms_spec += t1;
+        *ms_corr += t2;
+        return GS_OK;
+    };
+    // ---- sweep 1: moments ----
+    for (int ai = 0; ai < na; ++ai) {
+        CK(cudaEventRecord(ea, ctx->stream));
+        TRY(pair_spectra(ctx, angles[ai], TS));
+        CK(cudaEventRecord(eb, ctx->stream));
+        for (int w = 0; w < nw; ++w) {
+            TRY(corr_rows(ctx, W + (size_t)w * l2, TS, R));
+            Norm1Stats e{s1 + (size_t)w * l2, s2 + (size_t)w * l2, l, N, (float)l2, sgn};
+            TRY(corr_cols(ctx, R, e));
+        }
+        CK(cudaEventRecord(ec, ctx->stream));
+        TRY(elapsed());
+    }
+    {
+        const long long n = l2 * nw;
+        k_norm1_moments<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(s1, s2, n, (float)N * (float)na);
+        ++ctx->counters.kernel_launches;
+        CKL();
+    }
+    // ---- sweep 2: z-scores, block maxima, picks ----
+    const long long nkeys = (long long)N * nblk;
+    std::vector<BlockPickDev> hp;
+    for (int ai = 0; ai < na; ++ai) {
+        CK(cudaEventRecord(ea, ctx->stream));
+        TRY(pair_spectra(ctx, angles[ai], TS));
+        CK(cudaEventRecord(eb, ctx->stream));
+        CK(cudaMemsetAsync(keys, 0, sizeof(unsigned long long) * nkeys * nw, ctx->stream));
+        CK(cudaMemsetAsync(ctx->count.p, 0, sizeof(unsigned long long), ctx->stream));
+        for (int w = 0; w < nw; ++w) {
+            TRY(corr_rows(ctx, W + (size_t)w * l2, TS, R));
+            Norm1Blocks e{s1 + (size_t)w * l2, s2 + (size_t)w * l2, keys + (size_t)w * nkeys, l, N, nblk,
+                          (float)l, sgn};
+            TRY(corr_cols(ctx, R, e));
+            k_norm1_compact<<<blocks_for(nkeys, 256), 256, 0, ctx->stream>>>(
+                keys + (size_t)w * nkeys, N, nblk, l, offx[w % bx], offy[w / bx], ctx->p.d_m, nx, ny, ctx->p.thres,
+                ((long long)ai * nw + w) * nkeys, P<BlockPickDev>(ctx->picks), P<unsigned long long>(ctx->count),
+                nkeys * nw);
+            ++ctx->counters.kernel_launches;
+            CKL();
+        }
+        CK(cudaEventRecord(ec, ctx->stream));
+        TRY(elapsed());
+        unsigned long long cnt = 0;
+        CK(cudaMemcpy(&cnt, ctx->count.p, sizeof cnt, cudaMemcpyDeviceToHost));
+        if (cnt) {
+            const size_t o = hp.size();
+            hp.resize(o + cnt);
+            CK(cudaMemcpy(hp.data() + o, ctx->picks.p, sizeof(BlockPickDev) * cnt, cudaMemcpyDeviceToHost));
+        }
+    }
+    std::sort(hp.begin(), hp.end(), [](const BlockPickDev& a, const BlockPickDev& b) { return a.key < b.key; });
+    out->resize(hp.size());
+    for (size_t k = 0; k < hp.size(); ++k) {
+        const long long u = hp[k].key / nblk;
+        const int J = (int)(u % N);
+        const int w = (int)((u / N) % nw);
+        const int ai = (int)(u / ((long long)N * nw));
+        gs_pick& o = (*out)[k];
+        o.angle_index = ai;
+        o.phi = printed_phi(angles[ai]);
+        o.window_x = w % bx;
+        o.window_y = w / bx;
+        o.template_index = J;
+        o.center_x = hp[k].cx;
+        o.center_y = hp[k].cy;
+        o.score = hp[k].score;
+    }
+    return GS_OK;
+}
+
 extern "C" {
 
 const char* gs_status_string(int s) {
@@ -386,7 +540,8 @@ static int validate_params(gs_ctx* ctx, const gs_params* p) {
     if (!(p->apix > 0) || !(p->phi_step > 0) || !(p->kk >= 0) || !(p->energy > 0) || !(p->cs >= 0) ||
         !(p->highres > 0) || !(p->lowres > 0) || !(p->d_m > 0))
         return set_err(ctx, GS_ERR_ARG, "required parameter missing or not positive");
-    if (p->norm_type != 0) return set_err(ctx, GS_ERR_UNSUPPORTED, "norm_type %d is not implemented", p->norm_type);
+    if (p->norm_type != 0 && p->norm_type != 1)
+        return set_err(ctx, GS_ERR_ARG, "norm_type must be 0 or 1 (got %d)", p->norm_type);
     if (p->precision != GS_PREC_FP32) return set_err(ctx, GS_ERR_UNSUPPORTED, "precision mode %d", p->precision);
     if (p->window_size <= 0) return set_err(ctx, GS_ERR_ARG, "window_size must be positive");
     if (360.0f / p->phi_step > 1e6f) return set_err(ctx, GS_ERR_ARG, "phistep too small");
@@ -402,6 +557,10 @@ int gs_set_templates(gs_ctx* ctx, const gs_params* p, const float* host_template
     CK(cudaSetDevice(ctx->device));
     const int l = adjust_padding(p->window_size, tx, ty);
     if (l % 2) return set_err(ctx, GS_ERR_UNSUPPORTED, "window size %d must be even", l);
+    // norm_type 1 reduces 1024-element blocks of the flat l x l map
+    // (GPU_func.cu:711-745 with the launch at main.cu:798)
+    if (p->norm_type == 1 && ((long long)l * l) % 1024)
+        return set_err(ctx, GS_ERR_UNSUPPORTED, "norm_type 1 needs window*window to be a multiple of 1024 (window %d)", l);
     ctx->have_tmpl = false;
     ctx->have_units = false;
     ctx->p = *p;
@@ -603,6 +762,35 @@ static int search_impl(gs_ctx* ctx, const float* d_mic, int nx, int ny, const gs
         CKL();
     }
     CK(cudaEventRecord(ev[1], ctx->stream));
+    ctx->have_units = false;
+
+    if (p.norm_type == 1) {
+        TRY(ensure(ctx, ctx->tspec, sizeof(float2) * l2 * Np));
+        TRY(ensure(ctx, ctx->scratch, sizeof(float2) * l2 * Np));
+        TRY(ensure(ctx, ctx->pstats, sizeof(double) * 2 * N));
+        TRY(ensure(ctx, ctx->coef, sizeof(float4) * Np));
+        float ms_spec = 0.0f, ms_corr = 0.0f;
+        std::vector<gs_pick> hv;
+        TRY(search_norm1(ctx, W, nx, ny, offx, offy, angles, &ms_spec, &ms_corr, &hv));
+        CK(cudaEventRecord(ev[3], ctx->stream));
+        CK(cudaEventSynchronize(ev[3]));
+        gs_pick* out = nullptr;
+        if (!hv.empty()) {
+            out = (gs_pick*)malloc(sizeof(gs_pick) * hv.size());
+            if (!out) return set_err(ctx, GS_ERR_OOM, "host allocation of %zu picks", hv.size());
+            memcpy(out, hv.data(), sizeof(gs_pick) * hv.size());
+        }
+        *picks = out;
+        *n_picks = hv.size();
+        float t_prep = 0, t_tot = 0;
+        cudaEventElapsedTime(&t_prep, ev[0], ev[1]);
+        cudaEventElapsedTime(&t_tot, ev[0], ev[3]);
+        const float t[GS_TIMING_COUNT] = {t_prep, ms_spec, ms_corr, t_tot, 0, 0, 0, 0};
+        memcpy(ctx->timings, t, sizeof t);
+        ctx->counters.searches += 1;
+        ctx->counters.units += (unsigned long long)total_units;
+        return GS_OK;
+    }
 
     // ---- angle loop (main.cu:1232-1257) ----
     TRY(ensure(ctx, ctx->tspec, sizeof(float2) * l2 * Np));
@@ -651,28 +839,8 @@ static int search_impl(gs_ctx* ctx, const float* d_mic, int nx, int ny, const gs
     CK(cudaEventCreate(&ec));
     struct EvGuard3 { cudaEvent_t a, b, c; ~EvGuard3() { cudaEventDestroy(a); cudaEventDestroy(b); cudaEventDestroy(c); } } eg3{ea, eb, ec};
     for (int ai = 0; ai < na; ++ai) {
-        const float e = angles[ai];
-        const double ang = (double)e * kPiRef / 180.0;
-        const float cose = (float)cos(ang), sine = (float)sin(ang);
         CK(cudaEventRecord(ea, ctx->stream));
-        CK(cudaMemsetAsync(ctx->pstats.p, 0, sizeof(double) * 2 * N, ctx->stream));
-        {
-            dim3 g(blocks_for(l2, 256, 32), Np);
-            k_pair_rotate<<<g, 256, 0, ctx->stream>>>(P<float>(ctx->tmpl), N, l, cose, sine, p.d_m, TS,
-                                                      P<double>(ctx->pstats));
-            ++ctx->counters.kernel_launches;
-            k_pair_coef<<<blocks_for(Np, 128), 128, 0, ctx->stream>>>(P<double>(ctx->pstats), N, l,
-                                                                       P<float4>(ctx->coef));
-            ++ctx->counters.kernel_launches;
-            CKL();
-        }
-        if (fast_ok(ctx, l)) {
-            TRY(run_fast<false, false>(ctx, l, Np, F16PairNorm{TS, P<float4>(ctx->coef), l, l2}));
-            TRY(run_fast<false, true>(ctx, l, Np, F16Complex<true>{TS, l, l2, (float)(1.0 / (double)l2)}));
-        } else {
-            TRY(run_fft<false>(ctx, l, rows_of(l, l), Np, IoPairNorm{TS, P<float4>(ctx->coef), l2}));
-            TRY(run_fft<false>(ctx, l, cols_of(l, l), Np, IoComplex{TS, (float)(1.0 / (double)l2)}));
-        }
+        TRY(pair_spectra(ctx, angles[ai], TS));
         CK(cudaEventRecord(eb, ctx->stream));
         if (persistent) {
             int* cnt = P<int>(ctx->dep_counters);
@@ -843,7 +1011,8 @@ int gs_search(gs_ctx* ctx, const float* host_micrograph, int nx, int ny, const g
 
 int gs_get_units(gs_ctx* ctx, gs_unit* host_out, size_t cap, size_t* n_out) {
     if (!ctx || !n_out) return set_err(ctx, GS_ERR_ARG, "null pointer");
-    if (!ctx->have_units) return set_err(ctx, GS_ERR_STATE, "no search has run");
+    if (!ctx->have_units)
+        return set_err(ctx, GS_ERR_STATE, "no norm_type 0 search has run (units are its per-template maxima)");
     const size_t total = (size_t)ctx->last_na * ctx->last_nw * ctx->last_nt;
     *n_out = total;
     if (!host_out) return GS_OK;

@@ -55,7 +55,8 @@ typedef struct gs_params {
     int window_size;   /* window_size: window l (default 320) */
     int overlap;       /* overlap between windows, px (default -1) */
     int phase_flip;    /* phase_flip 0/1 (default 0) */
-    int norm_type;     /* norm_type: only 0 is implemented (default 0) */
+    int norm_type;     /* norm_type: 0 = peak / sigma per map, 1 = per-pixel
+                          z-score over all templates and angles (default 0) */
     int invert;        /* invert 0/1 (default 0) */
     float ampconst;    /* amplitude contrast (fixed 0.07 in the reference) */
     float a, b, b2;    /* noise-curve constants (DataReader.h:25) */
@@ -128,11 +129,15 @@ int gs_set_templates(struct gs_ctx* ctx, const gs_params* p, const float* host_t
 /* Geometry of a search of an nx x ny micrograph with the loaded templates. */
 int gs_get_geometry(struct gs_ctx* ctx, int nx, int ny, gs_geometry* out);
 
-/* One micrograph, norm_type 0.  Replaces init_d_image +
- * split_normalize_image + fft_on_img + the angle loop of rotateTemplate and
- * pickPartcles_IMG_NORM (main.cu:523-894, 1230-1257).  Picks come back in
- * the reference's line order (angle, window row, window column, template);
- * *picks is allocated by the library, release it with gs_picks_free.
+/* One micrograph.  Replaces init_d_image + split_normalize_image +
+ * fft_on_img + the angle loop of rotateTemplate and pickPartcles_IMG_NORM
+ * (main.cu:523-894, 1230-1257) for norm_type 0, and compute_CCG_sum +
+ * compute_CCG_mean + pickPartcles_CCG_NORM (main.cu:718-821, 1170-1229) for
+ * norm_type 1.  Picks come back in the reference's line order (angle,
+ * window row, window column, template; for norm_type 1 then the 1024-element
+ * block of the map); *picks is allocated by the library, release it with
+ * gs_picks_free.  norm_type 1 needs window * window to be a multiple of 1024
+ * (checked by gs_set_templates: GS_ERR_UNSUPPORTED).
  * host_micrograph: ny x nx float32 row-major. */
 int gs_search(struct gs_ctx* ctx, const float* host_micrograph, int nx, int ny,
               const gs_ctf* ctf, gs_pick** picks, size_t* n_picks);
@@ -143,7 +148,8 @@ int gs_search_device(struct gs_ctx* ctx, const float* device_micrograph, int nx,
                      const gs_ctf* ctf, gs_pick** picks, size_t* n_picks);
 
 /* Copy the dense per-unit table of the last search (n_angles x n_windows x
- * n_templates, that order) into host memory; cap is the element capacity. */
+ * n_templates, that order) into host memory; cap is the element capacity.
+ * Only a norm_type 0 search produces it (GS_ERR_STATE otherwise). */
 int gs_get_units(struct gs_ctx* ctx, gs_unit* host_out, size_t cap, size_t* n_out);
 
 void gs_picks_free(gs_pick* picks);

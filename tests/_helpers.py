@@ -18,6 +18,8 @@ from gisspa_b200 import formats, synth  # noqa: E402
 
 SMALL_CASES = ["small_pf1_all", "small_pf0_invert_astig", "small_astig_pf1_all",
                "pad_adjust_two_mics"]
+# norm_type 1 (per-pixel z-scores, 1024-element blocks)
+NORM1_CASES = ["norm1_small", "norm1_fast512"]
 
 # scores of the FP32 CUDA path against the FP64 oracle / the reference
 SCORE_RTOL = 1e-4

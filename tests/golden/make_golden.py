@@ -62,6 +62,16 @@ CASES = {
                                  defocus=(1.0, 2.0), astig_A=300.0, n_micrographs=2,
                                  threshold=4.0),
                             {}),
+    # norm_type 1: per-pixel z-scores over all templates and angles, 1024-element blocks
+    "norm1_small": (dict(seed=15, nx=448, ny=384, n_templates=5, tsize=64, n_particles=3,
+                         snr=0.4, n_blobs=60, ball_radius=20.0, phistep=45.0, diameter=48.0,
+                         window=128, overlap=32, threshold=3.4),
+                    {"norm_type": 1}),
+    # norm_type 1 at a window of 512 = 16 x 32 (the specialised FFT kernels)
+    "norm1_fast512": (dict(seed=16, nx=1100, ny=960, n_templates=5, tsize=120, n_particles=4,
+                           snr=0.4, n_blobs=80, ball_radius=36.0, phistep=45.0, diameter=100.0,
+                           window=512, overlap=100, threshold=3.6),
+                      {"norm_type": 1}),
     # the small benchmark workload itself (1024^2, 50 x 128^2 templates, 72 angles)
     "bench_small": (dict(synth.config_small(seed=0)), {"threshold": 6.0}),
 }

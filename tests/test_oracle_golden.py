@@ -23,7 +23,7 @@ def _run_oracle(name, tmp_path):
         os.chdir(cwd)
 
 
-@pytest.mark.parametrize("name", H.SMALL_CASES)
+@pytest.mark.parametrize("name", H.SMALL_CASES + H.NORM1_CASES)
 def test_oracle_matches_reference(name, tmp_path):
     gold = H.load_golden(name)
     assert gold["returncode"] == 0
