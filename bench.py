@@ -225,6 +225,13 @@ def cpu_baseline(ds, kw, geom) -> dict:
 # ---------------------------------------------------------------------------
 # our implementation
 # ---------------------------------------------------------------------------
+# gs_params.precision: FP32 CUDA cores, or the N2-point DFT stage on the
+# tensor cores with split 16-bit operands (include/gisspa.h GS_PREC_*)
+PRECISION_MODES = {"fp32": 0, "tc-bf16": 1, "tc-fp16": 2}
+DTYPES = {"fp32": "f32", "tc-bf16": "bf16 hi+lo split, f32 accumulate",
+          "tc-fp16": "fp16 hi+lo split, f32 accumulate"}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import gisspa_b200 as G
@@ -242,6 +249,7 @@ def run_ours(args, rank, world, local_rank):
     params = params_for(ds, kw)
     if args.phistep:
         params.phi_step = args.phistep
+    params.precision = PRECISION_MODES[args.precision]
     ctx = G.Context(local_rank)
     t0 = time.perf_counter()
     ctx.set_templates(params, ds.templates, ctf)
@@ -337,7 +345,7 @@ def run_ours(args, rank, world, local_rank):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None, "dtype": DTYPES[args.precision], "data": "synthetic",
         "config": {"workload": ("full-size single micrograph 5760x4092, 2000 templates 200x200, "
                                 "72 angles, window 720 overlap 200" if args.workload == "full"
                                 else "small micrograph 1024x1024, 50 templates 128x128, 72 angles, "
@@ -447,6 +455,8 @@ def main() -> int:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["full", "small"], default="full")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", choices=sorted(PRECISION_MODES), default="fp32",
+                    help="arithmetic of the correlation's N2-point DFT stage")
     # profiling aids (smaller captures); a line produced with them names the reduced workload
     ap.add_argument("--templates", type=int, default=None, help="use only the first N templates")
     ap.add_argument("--phistep", type=float, default=None, help="override the in-plane angle step")

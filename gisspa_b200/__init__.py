@@ -15,7 +15,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
-from typing import Optional, Sequence, Tuple
+from typing import List, Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -70,7 +70,7 @@ EXPORTS = ("gs_status_string", "gs_version", "gs_params_default", "gs_ctx_create
            "gs_ctx_destroy", "gs_ctx_last_error", "gs_set_templates", "gs_get_geometry",
            "gs_search", "gs_search_device", "gs_get_units", "gs_picks_free", "gs_get_timings",
            "gs_get_stats", "gs_set_kernel_timing", "gs_set_option",
-           "gs_correlate_window_noalloc")
+           "gs_correlate_window_noalloc", "gs_search_batch", "gs_get_tuning")
 
 _lib_handle = None
 
@@ -115,6 +115,11 @@ def load_library(path: Optional[str] = None) -> C.CDLL:
     lib.gs_correlate_window_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int,
                                                 C.c_float, C.c_void_p, C.c_void_p]
     lib.gs_get_stats.argtypes = [vp, C.POINTER(GsStats)]
+    lib.gs_search_batch.argtypes = [vp, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_int),
+                                    C.POINTER(C.c_int), C.POINTER(GsCtf),
+                                    C.POINTER(C.POINTER(GsPick)), C.POINTER(C.c_size_t),
+                                    C.POINTER(C.c_size_t)]
+    lib.gs_get_tuning.argtypes = [vp, C.POINTER(C.c_int)]
     if path is None:
         _lib_handle = lib
     return lib
@@ -211,6 +216,47 @@ class Context:
                                         C.byref(_ctf(ctf)), C.byref(ptr), C.byref(n)), "gs_search")
         return self._picks(ptr, n.value)
 
+    def search_batch(self, micrographs, ctfs) -> List[np.ndarray]:
+        """gs_search_batch: one search over several micrographs (sizes may
+        differ); returns each micrograph's picks."""
+        ms = [np.ascontiguousarray(m, dtype=np.float32) for m in micrographs]
+        n = len(ms)
+        if n == 0 or len(ctfs) != n:
+            raise ValueError("need one CTF per micrograph")
+        ptrs = (C.c_void_p * n)(*[m.ctypes.data for m in ms])
+        nx = (C.c_int * n)(*[m.shape[1] for m in ms])
+        ny = (C.c_int * n)(*[m.shape[0] for m in ms])
+        cs = (GsCtf * n)(*[_ctf(c) for c in ctfs])
+        per = (C.c_size_t * n)()
+        ptr = C.POINTER(GsPick)()
+        tot = C.c_size_t()
+        self._check(self._lib.gs_search_batch(self._h, n, ptrs, nx, ny, cs, C.byref(ptr),
+                                              C.byref(tot), per), "gs_search_batch")
+        allp = self._picks(ptr, tot.value)
+        out, k = [], 0
+        for m in range(n):
+            out.append(allp[k:k + per[m]].copy())
+            k += per[m]
+        return out
+
+    def set_graph(self, enable: bool) -> None:
+        """Capture the angle loop as one CUDA graph (GS_OPT_GRAPH)."""
+        self._check(self._lib.gs_set_option(self._h, 7, 1 if enable else 0), "gs_set_option")
+
+    def set_autotune(self, enable: bool) -> None:
+        """Tune the persistent kernel's scheduling on first use (GS_OPT_AUTOTUNE)."""
+        self._check(self._lib.gs_set_option(self._h, 8, 1 if enable else 0), "gs_set_option")
+
+    def set_corr_ctas(self, per_sm: int) -> None:
+        """Resident CTAs per SM of the persistent kernel (0 = as many as fit)."""
+        self._check(self._lib.gs_set_option(self._h, 6, int(per_sm)), "gs_set_option")
+
+    def tuning(self) -> Tuple[int, int, int, int]:
+        """(ring slots, lag, window block, CTAs per SM) of the last search."""
+        t = (C.c_int * 4)()
+        self._check(self._lib.gs_get_tuning(self._h, t), "gs_get_tuning")
+        return tuple(t[:])
+
     def search_device(self, dev_ptr: int, nx: int, ny: int, ctf) -> np.ndarray:
         ptr = C.POINTER(GsPick)()
         n = C.c_size_t()
@@ -288,11 +334,13 @@ def correlate_window_noalloc(d_window_spectrum: int, d_pair_spectra: int, n_temp
         raise GisspaError(st, "gs_correlate_window_noalloc(l=%d, n_templates=%d)" % (l, n_templates))
 
 
-def run_config(config_path: str, device: Optional[int] = None, return_units: bool = False):
+def run_config(config_path: str, device: Optional[int] = None, return_units: bool = False,
+               precision: int = 0):
     """Python mirror of the drop-in driver (main.cu:1025-1269 behaviour) over
     the C ABI: returns the output lines (and optionally the dense per-unit
     tables, one per micrograph).  Paths resolve relative to the current
-    directory, as in the reference."""
+    directory, as in the reference.  ``precision`` selects the arithmetic of
+    the correlation's DFT stage (GS_PREC_*, no config-file counterpart)."""
     from . import formats
     cfg = formats.read_config(config_path)
     missing = formats.missing_required(cfg)
@@ -309,6 +357,7 @@ def run_config(config_path: str, device: Optional[int] = None, return_units: boo
     if first is None:
         raise IOError("entry %d of %s not found" % (cfg.first, cfg.inlst))
     params = params_from_config(cfg)
+    params.precision = precision
     lines = []
     tables = []
     with Context(cfg.device_id if device is None else device) as ctx:

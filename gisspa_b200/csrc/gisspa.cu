@@ -10,6 +10,7 @@
 #include "fastfft.cuh"
 #include "kernels.cuh"
 #include "norm1.cuh"
+#include "tccorr.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -37,6 +38,14 @@ struct DBuf {
 
 }  // namespace
 
+struct CorrTuningSaved {
+    int slots, lag, window_block, ctas;
+};
+
+namespace {
+
+}  // namespace
+
 struct gs_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -60,6 +69,13 @@ struct gs_ctx {
     bool two_pass = false;
     int window_block = 4;
     int corr_slots = 16, corr_lag = 6;
+    int corr_ctas = 0;                 // resident CTAs per SM of the persistent kernels (0 = as many as fit)
+    int corr_ctas_override = 0;        // value used by the launch in progress
+    bool use_graph = false;            // capture the angle loop as one CUDA graph
+    bool autotune = false;             // tune the persistent kernels' scheduling on first use
+    std::map<long long, struct CorrTuningSaved> tuned;
+    int last_tuning[4] = {0, 0, 0, 0};
+    unsigned long long graph_kernel_launches = 0;
     DBuf unit_wp, dep_counters, pacc, flags;
     std::vector<cudaEvent_t> kev;  // pool of events for per-kernel timing
     gs_stats counters{0, 0, 0};
@@ -225,6 +241,7 @@ int launch_corr_n2(gs_ctx* ctx, const CorrArgs& a, long long total_items) {
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
     if (per_sm < 1) return set_err(ctx, GS_ERR_UNSUPPORTED, "persistent kernel does not fit on an SM");
+    if (ctx->corr_ctas_override > 0) per_sm = std::min(per_sm, ctx->corr_ctas_override);
     const long long grid = std::min<long long>((long long)nsm * per_sm, total_items);
     kern<<<(unsigned)grid, 256, smem, ctx->stream>>>(a);
     ++ctx->counters.kernel_launches;
@@ -238,6 +255,38 @@ int launch_corr(gs_ctx* ctx, int l, const CorrArgs& a, long long total_items) {
         case 45: return launch_corr_n2<45>(ctx, a, total_items);
         case 48: return launch_corr_n2<48>(ctx, a, total_items);
         default: return set_err(ctx, GS_ERR_UNSUPPORTED, "no persistent kernel for %d", l);
+    }
+}
+
+template <int N2, bool kBf16>
+int launch_corr_tc_n2(gs_ctx* ctx, const CorrArgs& a, long long total_items) {
+    using C = TcCfg<N2, kBf16>;
+    auto kern = k_corr_tc<N2, kBf16>;
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::bytes));
+    int per_sm = 0, nsm = 0, dev = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTcThreads, C::bytes));
+    if (per_sm < 1) return set_err(ctx, GS_ERR_UNSUPPORTED, "tensor-core kernel does not fit on an SM");
+    // TMEM: every resident CTA holds tmem_cols of the SM's 512 columns
+    per_sm = std::min(per_sm, (int)(512 / C::tmem_cols));
+    if (ctx->corr_ctas_override > 0) per_sm = std::min(per_sm, ctx->corr_ctas_override);
+    const long long grid = std::min<long long>((long long)nsm * per_sm, total_items);
+    kern<<<(unsigned)grid, kTcThreads, C::bytes, ctx->stream>>>(a);
+    ++ctx->counters.kernel_launches;
+    CKL();
+    return GS_OK;
+}
+
+// Persistent correlation with the tensor-core N2-point stage (tccorr.cuh).
+int launch_corr_tc(gs_ctx* ctx, int l, bool bf16, const CorrArgs& a) {
+    const int T = l / 8;
+    const long long total = (long long)(a.nu + a.lag) * 2 * T;
+    switch (l / 16) {
+        case 32: return bf16 ? launch_corr_tc_n2<32, true>(ctx, a, total) : launch_corr_tc_n2<32, false>(ctx, a, total);
+        case 45: return bf16 ? launch_corr_tc_n2<45, true>(ctx, a, total) : launch_corr_tc_n2<45, false>(ctx, a, total);
+        case 48: return bf16 ? launch_corr_tc_n2<48, true>(ctx, a, total) : launch_corr_tc_n2<48, false>(ctx, a, total);
+        default: return set_err(ctx, GS_ERR_UNSUPPORTED, "no tensor-core kernel for window %d", l);
     }
 }
 
@@ -542,7 +591,13 @@ static int validate_params(gs_ctx* ctx, const gs_params* p) {
         return set_err(ctx, GS_ERR_ARG, "required parameter missing or not positive");
     if (p->norm_type != 0 && p->norm_type != 1)
         return set_err(ctx, GS_ERR_ARG, "norm_type must be 0 or 1 (got %d)", p->norm_type);
-    if (p->precision != GS_PREC_FP32) return set_err(ctx, GS_ERR_UNSUPPORTED, "precision mode %d", p->precision);
+    if (p->precision != GS_PREC_FP32 && p->precision != GS_PREC_TC_BF16 && p->precision != GS_PREC_TC_FP16)
+        return set_err(ctx, GS_ERR_ARG, "unknown precision mode %d", p->precision);
+    if (p->precision != GS_PREC_FP32 && p->norm_type != 0)
+        return set_err(ctx, GS_ERR_UNSUPPORTED, "tensor-core precision modes need norm_type 0");
+    if (p->precision == GS_PREC_TC_FP16 && p->phase_flip != 1)
+        return set_err(ctx, GS_ERR_UNSUPPORTED,
+                       "GS_PREC_TC_FP16 needs phase_flip 1 (amplitude-normalised spectra keep the data in FP16 range)");
     if (p->window_size <= 0) return set_err(ctx, GS_ERR_ARG, "window_size must be positive");
     if (360.0f / p->phi_step > 1e6f) return set_err(ctx, GS_ERR_ARG, "phistep too small");
     return GS_OK;
@@ -654,27 +709,31 @@ int gs_get_geometry(gs_ctx* ctx, int nx, int ny, gs_geometry* out) {
     return GS_OK;
 }
 
-static int search_impl(gs_ctx* ctx, const float* d_mic, int nx, int ny, const gs_ctf* ctf, gs_pick** picks,
-                       size_t* n_picks) {
+// One micrograph of a search: its pixels, CTF, geometry, and where its
+// windows sit in the window-spectrum array (windows [w0, w0 + nw)).
+struct MicPlan {
+    const float* host = nullptr;  // host pixels, copied to the device first
+    const float* dev = nullptr;   // or device pixels
+    int nx = 0, ny = 0, bx = 0, by = 0, nw = 0, w0 = 0;
+    gs_ctf ctf{};
+    std::vector<int> offx, offy;
+};
+
+// Micrograph preprocessing and its window spectra (init_d_image +
+// split_normalize_image + fft_on_img, main.cu:523-655, 758-769), written to
+// W[w0 .. w0 + nw).
+static int prep_micrograph(gs_ctx* ctx, const MicPlan& mp, float2* W) {
     const gs_params& p = ctx->p;
     const int l = ctx->l;
     const long long l2 = (long long)l * l;
-    const int N = ctx->ntmpl;
-    const int Np = (N + 1) / 2;
+    const int nx = mp.nx, ny = mp.ny, bx = mp.bx, by = mp.by, nw = mp.nw;
     const long long npix = (long long)nx * ny;
-    if (l - p.overlap <= 0) return set_err(ctx, GS_ERR_ARG, "overlap must be smaller than the window");
-    if (std::max(nx, ny) / 2 > 1 << 20) return set_err(ctx, GS_ERR_UNSUPPORTED, "micrograph too large");
-    const std::vector<int> offx = window_offsets(nx, l, p.overlap), offy = window_offsets(ny, l, p.overlap);
-    const int bx = (int)offx.size(), by = (int)offy.size(), nw = bx * by;
-    const std::vector<float> angles = angle_list(p.phi_step);
-    const int na = (int)angles.size();
-    const long long total_units = (long long)na * nw * N;
-
-    cudaEvent_t ev[4];
-    for (auto& e : ev) CK(cudaEventCreate(&e));
-    struct EvGuard { cudaEvent_t* e; ~EvGuard() { for (int i = 0; i < 4; ++i) cudaEventDestroy(e[i]); } } evg{ev};
-    CK(cudaEventRecord(ev[0], ctx->stream));
-
+    const float* d_mic = mp.dev;
+    if (mp.host) {
+        TRY(ensure(ctx, ctx->in, sizeof(float) * npix));
+        CK(cudaMemcpyAsync(ctx->in.p, mp.host, sizeof(float) * npix, cudaMemcpyHostToDevice, ctx->stream));
+        d_mic = P<float>(ctx->in);
+    }
     // ---- micrograph: init_d_image (main.cu:523-586) ----
     TRY(ensure(ctx, ctx->q, sizeof(float) * 2 * npix));
     TRY(ensure(ctx, ctx->cimg, sizeof(float2) * npix));
@@ -696,7 +755,7 @@ static int search_impl(gs_ctx* ctx, const float* d_mic, int nx, int ny, const gs
     float2* C = P<float2>(ctx->cimg);
     TRY(run_fft<false>(ctx, nx, rows_of(nx, ny), 1, IoComplex{C, 1.0f}));
     TRY(run_fft<false>(ctx, ny, cols_of(nx, ny), 1, IoComplex{C, (float)(1.0 / (double)npix)}));
-    CtfDev cm = make_ctf(p, *ctf, l, nullptr);
+    CtfDev cm = make_ctf(p, mp.ctf, l, nullptr);
     if (p.phase_flip == 1) {
         CK(cudaMemsetAsync(ctx->ra.p, 0, sizeof(double) * ns, ctx->stream));
         CK(cudaMemsetAsync(ctx->rb.p, 0, sizeof(unsigned) * ns, ctx->stream));
@@ -727,107 +786,217 @@ static int search_impl(gs_ctx* ctx, const float* d_mic, int nx, int ny, const gs
 
     // ---- windows: split_normalize_image + fft_on_img (main.cu:588-655, 758-769) ----
     TRY(ensure(ctx, ctx->off, sizeof(int) * (bx + by)));
-    std::vector<int> offs(offx);
-    offs.insert(offs.end(), offy.begin(), offy.end());
+    std::vector<int> offs(mp.offx);
+    offs.insert(offs.end(), mp.offy.begin(), mp.offy.end());
     CK(cudaMemcpyAsync(ctx->off.p, offs.data(), sizeof(int) * offs.size(), cudaMemcpyHostToDevice, ctx->stream));
     const int* d_offx = P<int>(ctx->off);
     const int* d_offy = d_offx + bx;
-    TRY(ensure(ctx, ctx->win, sizeof(float2) * l2 * nw));
-    float2* W = P<float2>(ctx->win);
+    float2* Wm = W + (size_t)mp.w0 * l2;
     {
         dim3 g(blocks_for(l2, 256, 256), nw);
-        k_extract_windows<<<g, 256, 0, ctx->stream>>>(P<float>(ctx->img), nx, ny, d_offx, d_offy, bx, l, W);
+        k_extract_windows<<<g, 256, 0, ctx->stream>>>(P<float>(ctx->img), nx, ny, d_offx, d_offy, bx, l, Wm);
         ++ctx->counters.kernel_launches;
         CKL();
     }
     if (fast_ok(ctx, l)) {
-        TRY(run_fast<false, false>(ctx, l, nw, F16Complex<false>{W, l, l2, 1.0f}));
-        TRY(run_fast<false, true>(ctx, l, nw, F16Complex<true>{W, l, l2, (float)(1.0 / (double)l2)}));
+        TRY(run_fast<false, false>(ctx, l, nw, F16Complex<false>{Wm, l, l2, 1.0f}));
+        TRY(run_fast<false, true>(ctx, l, nw, F16Complex<true>{Wm, l, l2, (float)(1.0 / (double)l2)}));
     } else {
-        TRY(run_fft<false>(ctx, l, rows_of(l, l), nw, IoComplex{W, 1.0f}));
-        TRY(run_fft<false>(ctx, l, cols_of(l, l), nw, IoComplex{W, (float)(1.0 / (double)l2)}));
+        TRY(run_fft<false>(ctx, l, rows_of(l, l), nw, IoComplex{Wm, 1.0f}));
+        TRY(run_fft<false>(ctx, l, cols_of(l, l), nw, IoComplex{Wm, (float)(1.0 / (double)l2)}));
     }
     if (p.phase_flip == 1) {
         TRY(ensure(ctx, ctx->wsum, sizeof(double) * 2 * nw));
         TRY(ensure(ctx, ctx->winv, sizeof(double) * nw));
         CK(cudaMemsetAsync(ctx->wsum.p, 0, sizeof(double) * 2 * nw, ctx->stream));
         dim3 g(blocks_for(l2 / 2, 256, 64), nw);
-        k_win_sumsq<<<g, 256, 0, ctx->stream>>>(W, l, P<double>(ctx->wsum));
+        k_win_sumsq<<<g, 256, 0, ctx->stream>>>(Wm, l, P<double>(ctx->wsum));
         ++ctx->counters.kernel_launches;
         k_inv_amp_norm<<<blocks_for(nw, 128), 128, 0, ctx->stream>>>(P<double>(ctx->wsum), nw, P<double>(ctx->winv));
         ++ctx->counters.kernel_launches;
         dim3 g2(blocks_for(l2, 256, 256), nw);
-        k_scale_images<<<g2, 256, 0, ctx->stream>>>(W, l2, P<double>(ctx->winv));
+        k_scale_images<<<g2, 256, 0, ctx->stream>>>(Wm, l2, P<double>(ctx->winv));
         ++ctx->counters.kernel_launches;
         CKL();
     }
-    CK(cudaEventRecord(ev[1], ctx->stream));
-    ctx->have_units = false;
+    return GS_OK;
+}
 
-    if (p.norm_type == 1) {
-        TRY(ensure(ctx, ctx->tspec, sizeof(float2) * l2 * Np));
-        TRY(ensure(ctx, ctx->scratch, sizeof(float2) * l2 * Np));
-        TRY(ensure(ctx, ctx->pstats, sizeof(double) * 2 * N));
-        TRY(ensure(ctx, ctx->coef, sizeof(float4) * Np));
-        float ms_spec = 0.0f, ms_corr = 0.0f;
-        std::vector<gs_pick> hv;
-        TRY(search_norm1(ctx, W, nx, ny, offx, offy, angles, &ms_spec, &ms_corr, &hv));
-        CK(cudaEventRecord(ev[3], ctx->stream));
-        CK(cudaEventSynchronize(ev[3]));
-        gs_pick* out = nullptr;
-        if (!hv.empty()) {
-            out = (gs_pick*)malloc(sizeof(gs_pick) * hv.size());
-            if (!out) return set_err(ctx, GS_ERR_OOM, "host allocation of %zu picks", hv.size());
-            memcpy(out, hv.data(), sizeof(gs_pick) * hv.size());
-        }
-        *picks = out;
-        *n_picks = hv.size();
-        float t_prep = 0, t_tot = 0;
-        cudaEventElapsedTime(&t_prep, ev[0], ev[1]);
-        cudaEventElapsedTime(&t_tot, ev[0], ev[3]);
-        const float t[GS_TIMING_COUNT] = {t_prep, ms_spec, ms_corr, t_tot, 0, 0, 0, 0};
-        memcpy(ctx->timings, t, sizeof t);
-        ctx->counters.searches += 1;
-        ctx->counters.units += (unsigned long long)total_units;
+// Scheduling of the persistent correlation: ring slots, lag, window block,
+// resident CTAs per SM (0 = as many as fit).
+struct CorrTuning {
+    int slots, lag, window_block, ctas;
+};
+
+// Unit order: blocks of window_block windows; inside a block, pair-major.
+static int upload_unit_order(gs_ctx* ctx, int NW, int Np, int wbk, int limit) {
+    std::vector<int2> wp;
+    wp.reserve((size_t)NW * Np);
+    wbk = std::max(1, wbk);
+    for (int w0 = 0; w0 < NW; w0 += wbk)
+        for (int pp = 0; pp < Np; ++pp)
+            for (int w = w0; w < std::min(NW, w0 + wbk); ++w) wp.push_back(make_int2(w, pp));
+    const size_t n = std::min(wp.size(), (size_t)limit);
+    TRY(ensure(ctx, ctx->unit_wp, sizeof(int2) * std::max<size_t>(1, wp.size())));
+    CK(cudaMemcpyAsync(ctx->unit_wp.p, wp.data(), sizeof(int2) * n, cudaMemcpyHostToDevice, ctx->stream));
+    // the host vector must outlive the (staged) copy
+    CK(cudaStreamSynchronize(ctx->stream));
+    return GS_OK;
+}
+
+// One persistent correlation launch over the first nu units (angle ai's
+// template-pair spectra already in TS), results to out.
+static int corr_launch(gs_ctx* ctx, const float2* W, const float2* TS, int nu, const CorrTuning& t, UnitOut* out) {
+    const int l = ctx->l;
+    const long long l2 = (long long)l * l;
+    int* cnt = P<int>(ctx->dep_counters);
+    CK(cudaMemsetAsync(cnt, 0, sizeof(int) * (2 * (size_t)nu + 4), ctx->stream));
+    CK(cudaMemsetAsync(ctx->pacc.p, 0, sizeof(UnitAcc) * 2 * (size_t)nu, ctx->stream));
+    CorrArgs ca;
+    ca.W = W; ca.P = TS; ca.R = P<float2>(ctx->scratch);
+    ca.unit_wp = P<int2>(ctx->unit_wp);
+    ca.done_rows = cnt; ca.done_cols = cnt + nu;
+    ca.acc = P<UnitAcc>(ctx->pacc);
+    ca.out = out;
+    ca.next_item = cnt + 2 * (size_t)nu;
+    ca.error = P<int>(ctx->flags);
+    ca.nu = nu; ca.ntmpl = ctx->ntmpl; ca.S = t.slots; ca.lag = t.lag; ca.L2 = l2;
+    // border interval of unshifted indices: X = (x + l/2) mod l is masked
+    // when X < d_m/4 or X > l - d_m/4 (GPU_func.cu:681)
+    {
+        const float q_lo = ctx->p.d_m / 4.0f, q_hi = (float)l - q_lo;
+        const int h = l / 2;
+        const int ya = (int)ceilf(q_lo), yb = (int)floorf(q_hi);
+        ca.yb0 = yb - h + 1;
+        ca.yb1 = ya + h - 1;
+        if (ca.yb1 < ca.yb0) { ca.yb0 = 1; ca.yb1 = 0; }
+    }
+    ctx->corr_ctas_override = t.ctas;
+    if (ctx->p.precision == GS_PREC_FP32) return launch_corr(ctx, l, ca, (long long)(nu + t.lag) * 2 * (l / 16));
+    return launch_corr_tc(ctx, l, ctx->p.precision == GS_PREC_TC_BF16, ca);
+}
+
+// Autotuner of the persistent correlation's scheduling (no reference
+// counterpart): coordinate descent over ring slots, lag, window block and
+// CTAs per SM, each candidate timed with CUDA events on angle 0 over the
+// first min(nu, 8192) units of its own unit order.  The result is cached
+// per (window, templates, windows, precision).
+static int autotune(gs_ctx* ctx, const float2* W, const float2* TS, int NW, CorrTuning* best) {
+    const int N = ctx->ntmpl, Np = (N + 1) / 2;
+    const long long key = (((long long)ctx->l * 1000003 + N) * 1000003 + NW) * 4 + ctx->p.precision;
+    auto it = ctx->tuned.find(key);
+    if (it != ctx->tuned.end()) {
+        *best = CorrTuning{it->second.slots, it->second.lag, it->second.window_block, it->second.ctas};
         return GS_OK;
     }
+    const int nu_full = Np * NW;
+    const int nu = std::min(nu_full, 8192);
+    std::vector<int> slots_c = {8, 12, 16, 24, 32}, lag_c = {2, 4, 6, 10}, wb_c = {1, 2, 4, 8}, ctas_c = {0, 1};
+    CorrTuning cur{ctx->corr_slots, ctx->corr_lag, ctx->window_block, 0};
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    struct G2 { cudaEvent_t a, b; ~G2() { cudaEventDestroy(a); cudaEventDestroy(b); } } g2{e0, e1};
+    int order_wb = -1;
+    auto time_of = [&](const CorrTuning& t, float* ms) -> int {
+        if (t.window_block != order_wb) {
+            TRY(upload_unit_order(ctx, NW, Np, t.window_block, nu));
+            order_wb = t.window_block;
+        }
+        UnitOut* out = P<UnitOut>(ctx->units);
+        TRY(corr_launch(ctx, W, TS, nu, t, out));  // warm-up
+        CK(cudaEventRecord(e0, ctx->stream));
+        TRY(corr_launch(ctx, W, TS, nu, t, out));
+        CK(cudaEventRecord(e1, ctx->stream));
+        CK(cudaEventSynchronize(e1));
+        CK(cudaEventElapsedTime(ms, e0, e1));
+        return GS_OK;
+    };
+    float best_ms = 0;
+    TRY(time_of(cur, &best_ms));
+    for (int pass = 0; pass < 4; ++pass) {
+        const std::vector<int>& cand = pass == 0 ? slots_c : pass == 1 ? lag_c : pass == 2 ? wb_c : ctas_c;
+        for (int v : cand) {
+            CorrTuning t = cur;
+            if (pass == 0) t.slots = v;
+            else if (pass == 1) t.lag = v;
+            else if (pass == 2) t.window_block = v;
+            else t.ctas = v;
+            if (t.lag >= t.slots) continue;
+            if (t.slots == cur.slots && t.lag == cur.lag && t.window_block == cur.window_block && t.ctas == cur.ctas)
+                continue;
+            float ms = 0;
+            TRY(time_of(t, &ms));
+            if (ms < best_ms) {
+                best_ms = ms;
+                cur = t;
+            }
+        }
+    }
+    int flag = 0;
+    CK(cudaMemcpy(&flag, ctx->flags.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) return set_err(ctx, GS_ERR_TIMEOUT, "correlation kernel: a bounded dependency wait gave up (autotuner)");
+    ctx->tuned[key] = CorrTuningSaved{cur.slots, cur.lag, cur.window_block, cur.ctas};
+    *best = cur;
+    return GS_OK;
+}
 
-    // ---- angle loop (main.cu:1232-1257) ----
+// Correlation of every window with every template over all angles (the
+// angle loop of main.cu:1232-1257): per angle the template-pair spectra, then
+// either one persistent launch over all (window, pair) units or per-window
+// row and column launches.  Results to ctx->units [angle][NW][N].
+static int correlate_all(gs_ctx* ctx, const float2* W, int NW, const std::vector<float>& angles, float* t_spec,
+                         float* t_corr, float kt[4]) {
+    const gs_params& p = ctx->p;
+    const int l = ctx->l;
+    const long long l2 = (long long)l * l;
+    const int N = ctx->ntmpl, Np = (N + 1) / 2;
+    const int na = (int)angles.size();
+    const long long total_units = (long long)na * NW * N;
+    const bool persistent = fast_ok(ctx, l) && !ctx->two_pass;
+    if (p.precision != GS_PREC_FP32 && !persistent)
+        return set_err(ctx, GS_ERR_UNSUPPORTED,
+                       "tensor-core precision needs window 512, 720 or 768 and the persistent path (window %d)", l);
+    const int nu = Np * NW;
+    if ((long long)(nu + 64) * 2 * (l / 8) >= (1ll << 31))
+        return set_err(ctx, GS_ERR_UNSUPPORTED, "too many (window, template pair) units in one search (%d)", nu);
     TRY(ensure(ctx, ctx->tspec, sizeof(float2) * l2 * Np));
-    TRY(ensure(ctx, ctx->scratch, sizeof(float2) * l2 * (fast_ok(ctx, l) && !ctx->two_pass ? ctx->corr_slots : Np)));
     TRY(ensure(ctx, ctx->pstats, sizeof(double) * 2 * N));
     TRY(ensure(ctx, ctx->coef, sizeof(float4) * Np));
     TRY(ensure(ctx, ctx->acc, sizeof(UnitAcc) * N));
     TRY(ensure(ctx, ctx->units, sizeof(UnitOut) * std::max<long long>(1, total_units)));
-    const bool persistent = fast_ok(ctx, l) && !ctx->two_pass;
-    const int nu = Np * nw;
-    const int corr_slots = ctx->corr_slots, corr_lag = ctx->corr_lag;
+    float2* TS = P<float2>(ctx->tspec);
+    UnitOut* units = P<UnitOut>(ctx->units);
+    FftPlan* plan = nullptr;
+    TRY(get_plan(ctx, l, &plan));  // before any capture: plan creation copies synchronously
+    CorrTuning tune{ctx->corr_slots, ctx->corr_lag, ctx->window_block, ctx->corr_ctas};
     if (persistent) {
-        // unit order: blocks of window_block windows; inside a block, pair-major
-        std::vector<int2> wp;
-        wp.reserve(nu);
-        const int wbk = std::max(1, ctx->window_block);
-        for (int w0 = 0; w0 < nw; w0 += wbk)
-            for (int pp = 0; pp < Np; ++pp)
-                for (int w = w0; w < std::min(nw, w0 + wbk); ++w) wp.push_back(make_int2(w, pp));
-        TRY(ensure(ctx, ctx->unit_wp, sizeof(int2) * nu));
-        CK(cudaMemcpyAsync(ctx->unit_wp.p, wp.data(), sizeof(int2) * nu, cudaMemcpyHostToDevice, ctx->stream));
         TRY(ensure(ctx, ctx->dep_counters, sizeof(int) * (2 * (size_t)nu + 4)));
         TRY(ensure(ctx, ctx->pacc, sizeof(UnitAcc) * 2 * (size_t)nu));
         TRY(ensure(ctx, ctx->flags, sizeof(int) * 4));
         CK(cudaMemsetAsync(ctx->flags.p, 0, sizeof(int) * 4, ctx->stream));
+        if (ctx->autotune) {
+            TRY(ensure(ctx, ctx->scratch, sizeof(float2) * l2 * 32));
+            TRY(pair_spectra(ctx, angles[0], TS));
+            TRY(autotune(ctx, W, TS, NW, &tune));
+        }
+        TRY(upload_unit_order(ctx, NW, Np, tune.window_block, nu));
+        TRY(ensure(ctx, ctx->scratch, sizeof(float2) * l2 * tune.slots));
+    } else {
+        TRY(ensure(ctx, ctx->scratch, sizeof(float2) * l2 * Np));
     }
-    float2* TS = P<float2>(ctx->tspec);
+    ctx->last_tuning[0] = tune.slots;
+    ctx->last_tuning[1] = tune.lag;
+    ctx->last_tuning[2] = tune.window_block;
+    ctx->last_tuning[3] = tune.ctas;
     float2* R = P<float2>(ctx->scratch);
     UnitAcc* acc = P<UnitAcc>(ctx->acc);
-    UnitOut* units = P<UnitOut>(ctx->units);
     const float q_lo = p.d_m / 4.0f;
     const float q_hi = (float)l - q_lo;
     const float sgn = ((l / 2) % 2 == 0) ? 1.0f : -1.0f;
-    float ms_spec = 0.0f, ms_corr = 0.0f, k1ms = 0.0f, k2ms = 0.0f;
-    long long k1n = 0, k2n = 0;
-    if (ctx->kernel_timing && (int)ctx->kev.size() < 4 * nw) {
-        while ((int)ctx->kev.size() < 4 * nw) {
+    const bool timing = ctx->kernel_timing && !ctx->use_graph;
+    if (timing && (int)ctx->kev.size() < 4 * NW) {
+        while ((int)ctx->kev.size() < 4 * NW) {
             cudaEvent_t e;
             CK(cudaEventCreate(&e));
             ctx->kev.push_back(e);
@@ -838,44 +1007,28 @@ static int search_impl(gs_ctx* ctx, const float* d_mic, int nx, int ny, const gs
     CK(cudaEventCreate(&eb));
     CK(cudaEventCreate(&ec));
     struct EvGuard3 { cudaEvent_t a, b, c; ~EvGuard3() { cudaEventDestroy(a); cudaEventDestroy(b); cudaEventDestroy(c); } } eg3{ea, eb, ec};
-    for (int ai = 0; ai < na; ++ai) {
-        CK(cudaEventRecord(ea, ctx->stream));
+    float k1ms = 0, k2ms = 0;
+    long long k1n = 0, k2n = 0;
+
+    // the work of one angle, enqueued on the context's stream
+    auto enqueue_angle = [&](int ai, bool rec) -> int {
+        if (rec) CK(cudaEventRecord(ea, ctx->stream));
         TRY(pair_spectra(ctx, angles[ai], TS));
-        CK(cudaEventRecord(eb, ctx->stream));
+        if (rec) CK(cudaEventRecord(eb, ctx->stream));
         if (persistent) {
-            int* cnt = P<int>(ctx->dep_counters);
-            CK(cudaMemsetAsync(cnt, 0, sizeof(int) * (2 * (size_t)nu + 4), ctx->stream));
-            CK(cudaMemsetAsync(ctx->pacc.p, 0, sizeof(UnitAcc) * 2 * (size_t)nu, ctx->stream));
-            CorrArgs ca;
-            ca.W = W; ca.P = TS; ca.R = R;
-            ca.unit_wp = P<int2>(ctx->unit_wp);
-            ca.done_rows = cnt; ca.done_cols = cnt + nu;
-            ca.acc = P<UnitAcc>(ctx->pacc);
-            ca.out = units + (size_t)ai * nw * N;
-            ca.next_item = cnt + 2 * (size_t)nu;
-            ca.error = P<int>(ctx->flags);
-            ca.nu = nu; ca.ntmpl = N; ca.S = corr_slots; ca.lag = corr_lag; ca.L2 = l2;
-            // border interval of unshifted indices: X = (x + l/2) mod l is masked
-            // when X < d_m/4 or X > l - d_m/4 (GPU_func.cu:681)
-            {
-                const int h = l / 2;
-                int ya = (int)ceilf(q_lo), yb = (int)floorf(q_hi);
-                ca.yb0 = yb - h + 1;
-                ca.yb1 = ya + h - 1;
-                if (ca.yb1 < ca.yb0) { ca.yb0 = 1; ca.yb1 = 0; }
-            }
-            if (ctx->kernel_timing) CK(cudaEventRecord(ctx->kev[0], ctx->stream));
-            TRY(launch_corr(ctx, l, ca, (long long)(nu + corr_lag) * 2 * (l / 16)));
-            if (ctx->kernel_timing) CK(cudaEventRecord(ctx->kev[1], ctx->stream));
+            if (timing) CK(cudaEventRecord(ctx->kev[0], ctx->stream));
+            TRY(corr_launch(ctx, W, TS, nu, tune, units + (size_t)ai * NW * N));
+            if (timing) CK(cudaEventRecord(ctx->kev[1], ctx->stream));
+            return GS_OK;
         }
-        for (int w = 0; w < nw && !persistent; ++w) {
+        for (int w = 0; w < NW; ++w) {
             CK(cudaMemsetAsync(acc, 0, sizeof(UnitAcc) * N, ctx->stream));
             const bool fast = fast_ok(ctx, l);
-            if (ctx->kernel_timing) CK(cudaEventRecord(ctx->kev[4 * w + 0], ctx->stream));
+            if (timing) CK(cudaEventRecord(ctx->kev[4 * w + 0], ctx->stream));
             if (fast) TRY(run_fast<true, false>(ctx, l, Np, F16Pass1{W + (size_t)w * l2, TS, R, l, l2}));
             else TRY(run_fft<true>(ctx, l, rows_of(l, l), Np, IoPass1{W + (size_t)w * l2, TS, R, l2}));
-            if (ctx->kernel_timing) CK(cudaEventRecord(ctx->kev[4 * w + 1], ctx->stream));
-            if (ctx->kernel_timing) CK(cudaEventRecord(ctx->kev[4 * w + 2], ctx->stream));
+            if (timing) CK(cudaEventRecord(ctx->kev[4 * w + 1], ctx->stream));
+            if (timing) CK(cudaEventRecord(ctx->kev[4 * w + 2], ctx->stream));
             if (fast) {
                 F16Pass2 io2;
                 io2.R = R; io2.acc = acc; io2.L = l; io2.ntmpl = N; io2.L2 = l2;
@@ -886,34 +1039,64 @@ static int search_impl(gs_ctx* ctx, const float* d_mic, int nx, int ny, const gs
                 io2.R = R; io2.acc = acc; io2.l = l; io2.ntmpl = N; io2.q_lo = q_lo; io2.q_hi = q_hi; io2.sgn = sgn;
                 TRY(run_fft<true>(ctx, l, cols_of(l, l), Np, io2));
             }
-            if (ctx->kernel_timing) CK(cudaEventRecord(ctx->kev[4 * w + 3], ctx->stream));
-            k_finalize<<<blocks_for(N, 128), 128, 0, ctx->stream>>>(acc, N, l,
-                                                                    units + ((size_t)ai * nw + w) * N);
+            if (timing) CK(cudaEventRecord(ctx->kev[4 * w + 3], ctx->stream));
+            k_finalize<<<blocks_for(N, 128), 128, 0, ctx->stream>>>(acc, N, l, units + ((size_t)ai * NW + w) * N);
             ++ctx->counters.kernel_launches;
             CKL();
         }
+        return GS_OK;
+    };
+
+    if (ctx->use_graph) {
+        // the whole angle loop as one CUDA graph: captured once, launched once
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        const unsigned long long launches0 = ctx->counters.kernel_launches;
+        CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        int st = GS_OK;
+        for (int ai = 0; ai < na && st == GS_OK; ++ai) st = enqueue_angle(ai, false);
+        const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
+        if (st != GS_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return st;
+        }
+        if (ce != cudaSuccess) return set_err(ctx, GS_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+        struct GGuard { cudaGraph_t g; cudaGraphExec_t* e; ~GGuard() { if (*e) cudaGraphExecDestroy(*e); cudaGraphDestroy(g); } } gg{graph, &exec};
+        CK(cudaGraphInstantiate(&exec, graph, 0));
+        ctx->graph_kernel_launches = ctx->counters.kernel_launches - launches0;
+        CK(cudaEventRecord(eb, ctx->stream));
+        CK(cudaGraphLaunch(exec, ctx->stream));
         CK(cudaEventRecord(ec, ctx->stream));
         CK(cudaEventSynchronize(ec));
-        float t1 = 0, t2 = 0;
-        cudaEventElapsedTime(&t1, ea, eb);
-        cudaEventElapsedTime(&t2, eb, ec);
-        ms_spec += t1;
-        ms_corr += t2;
-        if (ctx->kernel_timing && persistent) {
-            float a = 0;
-            cudaEventElapsedTime(&a, ctx->kev[0], ctx->kev[1]);
-            k1ms += a;
-            k1n += 1;
-        } else if (ctx->kernel_timing) {
-            for (int w = 0; w < nw; ++w) {
-                float a = 0, b = 0;
-                cudaEventElapsedTime(&a, ctx->kev[4 * w + 0], ctx->kev[4 * w + 1]);
-                cudaEventElapsedTime(&b, ctx->kev[4 * w + 2], ctx->kev[4 * w + 3]);
+        float t = 0;
+        cudaEventElapsedTime(&t, eb, ec);
+        *t_corr += t;
+    } else {
+        for (int ai = 0; ai < na; ++ai) {
+            TRY(enqueue_angle(ai, true));
+            CK(cudaEventRecord(ec, ctx->stream));
+            CK(cudaEventSynchronize(ec));
+            float t1 = 0, t2 = 0;
+            cudaEventElapsedTime(&t1, ea, eb);
+            cudaEventElapsedTime(&t2, eb, ec);
+            *t_spec += t1;
+            *t_corr += t2;
+            if (timing && persistent) {
+                float a = 0;
+                cudaEventElapsedTime(&a, ctx->kev[0], ctx->kev[1]);
                 k1ms += a;
-                k2ms += b;
+                k1n += 1;
+            } else if (timing) {
+                for (int w = 0; w < NW; ++w) {
+                    float a = 0, b = 0;
+                    cudaEventElapsedTime(&a, ctx->kev[4 * w + 0], ctx->kev[4 * w + 1]);
+                    cudaEventElapsedTime(&b, ctx->kev[4 * w + 2], ctx->kev[4 * w + 3]);
+                    k1ms += a;
+                    k2ms += b;
+                }
+                k1n += NW;
+                k2n += NW;
             }
-            k1n += nw;
-            k2n += nw;
         }
     }
     if (persistent) {
@@ -922,19 +1105,32 @@ static int search_impl(gs_ctx* ctx, const float* d_mic, int nx, int ny, const gs
         CK(cudaStreamSynchronize(ctx->stream));
         if (flag) return set_err(ctx, GS_ERR_TIMEOUT, "correlation kernel: a bounded dependency wait gave up");
     }
-    ctx->last_na = na;
-    ctx->last_nw = nw;
-    ctx->last_nt = N;
-    ctx->have_units = true;
+    kt[0] = k1ms;
+    kt[1] = (float)k1n;
+    kt[2] = k2ms;
+    kt[3] = (float)k2n;
+    return GS_OK;
+}
 
-    // ---- picks (main.cu:869-891), reference order restored by sorting ----
-    TRY(ensure(ctx, ctx->picks, sizeof(PickDev) * std::max<long long>(1, total_units)));
+// Threshold picks of one micrograph (main.cu:869-891), in the reference's
+// line order (angle, window row, window column, template).
+static int compact_picks(gs_ctx* ctx, const MicPlan& mp, int NW, const std::vector<float>& angles,
+                         std::vector<gs_pick>* out) {
+    const gs_params& p = ctx->p;
+    const int N = ctx->ntmpl, na = (int)angles.size();
+    const long long total = (long long)na * mp.nw * N;
+    TRY(ensure(ctx, ctx->picks, sizeof(PickDev) * std::max<long long>(1, total)));
     TRY(ensure(ctx, ctx->count, sizeof(unsigned long long)));
+    TRY(ensure(ctx, ctx->off, sizeof(int) * (mp.bx + mp.by)));
+    std::vector<int> offs(mp.offx);
+    offs.insert(offs.end(), mp.offy.begin(), mp.offy.end());
+    CK(cudaMemcpyAsync(ctx->off.p, offs.data(), sizeof(int) * offs.size(), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemsetAsync(ctx->count.p, 0, sizeof(unsigned long long), ctx->stream));
-    if (total_units > 0) {
-        k_compact<<<blocks_for(total_units, 256), 256, 0, ctx->stream>>>(
-            units, total_units, nw, N, bx, d_offx, d_offy, l, p.d_m, nx, ny, p.thres, P<PickDev>(ctx->picks),
-            P<unsigned long long>(ctx->count), total_units);
+    if (total > 0) {
+        const int* d_offx = P<int>(ctx->off);
+        k_compact<<<blocks_for(total, 256), 256, 0, ctx->stream>>>(
+            P<UnitOut>(ctx->units), total, mp.nw, N, mp.bx, d_offx, d_offx + mp.bx, ctx->l, p.d_m, mp.nx, mp.ny,
+            p.thres, P<PickDev>(ctx->picks), P<unsigned long long>(ctx->count), total, NW, mp.w0);
         ++ctx->counters.kernel_launches;
         CKL();
     }
@@ -943,44 +1139,113 @@ static int search_impl(gs_ctx* ctx, const float* d_mic, int nx, int ny, const gs
     CK(cudaStreamSynchronize(ctx->stream));
     std::vector<PickDev> hp(cnt);
     if (cnt) CK(cudaMemcpy(hp.data(), ctx->picks.p, sizeof(PickDev) * cnt, cudaMemcpyDeviceToHost));
+    std::sort(hp.begin(), hp.end(), [](const PickDev& a, const PickDev& b) { return a.unit < b.unit; });
+    out->resize(cnt);
+    for (size_t k = 0; k < cnt; ++k) {
+        const long long u = hp[k].unit;
+        const int J = (int)(u % N);
+        const int w = (int)((u / N) % mp.nw);
+        const int ai = (int)(u / ((long long)N * mp.nw));
+        gs_pick& o = (*out)[k];
+        o.angle_index = ai;
+        o.phi = printed_phi(angles[ai]);
+        o.window_x = w % mp.bx;
+        o.window_y = w / mp.bx;
+        o.template_index = J;
+        o.center_x = hp[k].cx;
+        o.center_y = hp[k].cy;
+        o.score = hp[k].score;
+    }
+    return GS_OK;
+}
+
+// A search over one or more micrographs with the loaded templates.  The
+// windows of all micrographs share one window-spectrum array and every angle's
+// template-pair spectra; each micrograph's picks come out in the reference's
+// order, micrographs in the given order.
+static int search_many(gs_ctx* ctx, std::vector<MicPlan>& mics, std::vector<std::vector<gs_pick>>* res) {
+    const gs_params& p = ctx->p;
+    const int l = ctx->l;
+    const long long l2 = (long long)l * l;
+    const int N = ctx->ntmpl;
+    if (l - p.overlap <= 0) return set_err(ctx, GS_ERR_ARG, "overlap must be smaller than the window");
+    int NW = 0;
+    for (MicPlan& mp : mics) {
+        if (std::max(mp.nx, mp.ny) / 2 > 1 << 20) return set_err(ctx, GS_ERR_UNSUPPORTED, "micrograph too large");
+        mp.offx = window_offsets(mp.nx, l, p.overlap);
+        mp.offy = window_offsets(mp.ny, l, p.overlap);
+        mp.bx = (int)mp.offx.size();
+        mp.by = (int)mp.offy.size();
+        mp.nw = mp.bx * mp.by;
+        mp.w0 = NW;
+        NW += mp.nw;
+    }
+    if (p.norm_type == 1 && mics.size() != 1)
+        return set_err(ctx, GS_ERR_UNSUPPORTED, "norm_type 1 searches one micrograph per call");
+    const std::vector<float> angles = angle_list(p.phi_step);
+    const int na = (int)angles.size();
+    const long long total_units = (long long)na * NW * N;
+    ctx->have_units = false;
+
+    cudaEvent_t ev[4];
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    struct EvGuard { cudaEvent_t* e; ~EvGuard() { for (int i = 0; i < 4; ++i) cudaEventDestroy(e[i]); } } evg{ev};
+    CK(cudaEventRecord(ev[0], ctx->stream));
+    TRY(ensure(ctx, ctx->win, sizeof(float2) * l2 * NW));
+    float2* W = P<float2>(ctx->win);
+    for (const MicPlan& mp : mics) TRY(prep_micrograph(ctx, mp, W));
+    CK(cudaEventRecord(ev[1], ctx->stream));
+
+    float t_spec = 0.0f, t_corr = 0.0f, kt[4] = {0, 0, 0, 0};
+    res->assign(mics.size(), std::vector<gs_pick>());
+    if (p.norm_type == 1) {
+        const int Np = (N + 1) / 2;
+        TRY(ensure(ctx, ctx->tspec, sizeof(float2) * l2 * Np));
+        TRY(ensure(ctx, ctx->scratch, sizeof(float2) * l2 * Np));
+        TRY(ensure(ctx, ctx->pstats, sizeof(double) * 2 * N));
+        TRY(ensure(ctx, ctx->coef, sizeof(float4) * Np));
+        const MicPlan& mp = mics[0];
+        TRY(search_norm1(ctx, W, mp.nx, mp.ny, mp.offx, mp.offy, angles, &t_spec, &t_corr, &(*res)[0]));
+    } else {
+        TRY(correlate_all(ctx, W, NW, angles, &t_spec, &t_corr, kt));
+        ctx->last_na = na;
+        ctx->last_nw = NW;
+        ctx->last_nt = N;
+        ctx->have_units = true;
+        for (size_t m = 0; m < mics.size(); ++m) TRY(compact_picks(ctx, mics[m], NW, angles, &(*res)[m]));
+    }
     CK(cudaEventRecord(ev[3], ctx->stream));
     CK(cudaEventSynchronize(ev[3]));
-    std::sort(hp.begin(), hp.end(), [](const PickDev& a, const PickDev& b) { return a.unit < b.unit; });
-    gs_pick* out = nullptr;
-    if (cnt) {
-        out = (gs_pick*)malloc(sizeof(gs_pick) * cnt);
-        if (!out) return set_err(ctx, GS_ERR_OOM, "host allocation of %llu picks", cnt);
-        for (size_t k = 0; k < cnt; ++k) {
-            const long long u = hp[k].unit;
-            const int J = (int)(u % N);
-            const int w = (int)((u / N) % nw);
-            const int ai = (int)(u / ((long long)N * nw));
-            gs_pick& o = out[k];
-            o.angle_index = ai;
-            o.phi = printed_phi(angles[ai]);
-            o.window_x = w % bx;
-            o.window_y = w / bx;
-            o.template_index = J;
-            o.center_x = hp[k].cx;
-            o.center_y = hp[k].cy;
-            o.score = hp[k].score;
-        }
-    }
-    *picks = out;
-    *n_picks = (size_t)cnt;
     float t_prep = 0, t_tot = 0;
     cudaEventElapsedTime(&t_prep, ev[0], ev[1]);
     cudaEventElapsedTime(&t_tot, ev[0], ev[3]);
-    ctx->timings[0] = t_prep;
-    ctx->timings[1] = ms_spec;
-    ctx->timings[2] = ms_corr;
-    ctx->timings[3] = t_tot;
-    ctx->timings[4] = k1ms;
-    ctx->timings[5] = (float)k1n;
-    ctx->timings[6] = k2ms;
-    ctx->timings[7] = (float)k2n;
+    const float t[GS_TIMING_COUNT] = {t_prep, t_spec, t_corr, t_tot, kt[0], kt[1], kt[2], kt[3]};
+    memcpy(ctx->timings, t, sizeof t);
     ctx->counters.searches += 1;
     ctx->counters.units += (unsigned long long)total_units;
+    return GS_OK;
+}
+
+// Concatenated picks in a library-owned array.
+static int hand_out(gs_ctx* ctx, const std::vector<std::vector<gs_pick>>& res, gs_pick** picks, size_t* n_picks,
+                    size_t* per_mic) {
+    size_t n = 0;
+    for (size_t m = 0; m < res.size(); ++m) {
+        if (per_mic) per_mic[m] = res[m].size();
+        n += res[m].size();
+    }
+    gs_pick* out = nullptr;
+    if (n) {
+        out = (gs_pick*)malloc(sizeof(gs_pick) * n);
+        if (!out) return set_err(ctx, GS_ERR_OOM, "host allocation of %zu picks", n);
+        size_t k = 0;
+        for (const auto& v : res) {
+            if (!v.empty()) memcpy(out + k, v.data(), sizeof(gs_pick) * v.size());
+            k += v.size();
+        }
+    }
+    *picks = out;
+    *n_picks = n;
     return GS_OK;
 }
 
@@ -992,7 +1257,14 @@ int gs_search_device(gs_ctx* ctx, const float* device_micrograph, int nx, int ny
     *n_picks = 0;
     if (!ctx->have_tmpl) return set_err(ctx, GS_ERR_STATE, "gs_set_templates must come first");
     CK(cudaSetDevice(ctx->device));
-    return search_impl(ctx, device_micrograph, nx, ny, ctf, picks, n_picks);
+    std::vector<MicPlan> mics(1);
+    mics[0].dev = device_micrograph;
+    mics[0].nx = nx;
+    mics[0].ny = ny;
+    mics[0].ctf = *ctf;
+    std::vector<std::vector<gs_pick>> res;
+    TRY(search_many(ctx, mics, &res));
+    return hand_out(ctx, res, picks, n_picks, nullptr);
 }
 
 int gs_search(gs_ctx* ctx, const float* host_micrograph, int nx, int ny, const gs_ctf* ctf, gs_pick** picks,
@@ -1003,10 +1275,54 @@ int gs_search(gs_ctx* ctx, const float* host_micrograph, int nx, int ny, const g
     *n_picks = 0;
     if (!ctx->have_tmpl) return set_err(ctx, GS_ERR_STATE, "gs_set_templates must come first");
     CK(cudaSetDevice(ctx->device));
-    const size_t bytes = sizeof(float) * (size_t)nx * ny;
-    TRY(ensure(ctx, ctx->in, bytes));
-    CK(cudaMemcpyAsync(ctx->in.p, host_micrograph, bytes, cudaMemcpyHostToDevice, ctx->stream));
-    return search_impl(ctx, P<float>(ctx->in), nx, ny, ctf, picks, n_picks);
+    std::vector<MicPlan> mics(1);
+    mics[0].host = host_micrograph;
+    mics[0].nx = nx;
+    mics[0].ny = ny;
+    mics[0].ctf = *ctf;
+    std::vector<std::vector<gs_pick>> res;
+    TRY(search_many(ctx, mics, &res));
+    return hand_out(ctx, res, picks, n_picks, nullptr);
+}
+
+int gs_search_batch(gs_ctx* ctx, int n_micrographs, const float* const* host_micrographs, const int* nx,
+                    const int* ny, const gs_ctf* ctfs, gs_pick** picks, size_t* n_picks, size_t* picks_per_micrograph) {
+    if (!ctx || n_micrographs <= 0 || !host_micrographs || !nx || !ny || !ctfs || !picks || !n_picks ||
+        !picks_per_micrograph)
+        return set_err(ctx, GS_ERR_ARG, "null pointer or empty batch");
+    *picks = nullptr;
+    *n_picks = 0;
+    for (int m = 0; m < n_micrographs; ++m) {
+        picks_per_micrograph[m] = 0;
+        if (!host_micrographs[m] || nx[m] <= 0 || ny[m] <= 0)
+            return set_err(ctx, GS_ERR_ARG, "micrograph %d: null pointer or empty", m);
+    }
+    if (!ctx->have_tmpl) return set_err(ctx, GS_ERR_STATE, "gs_set_templates must come first");
+    CK(cudaSetDevice(ctx->device));
+    std::vector<std::vector<gs_pick>> res(n_micrographs);
+    if (ctx->p.norm_type == 1) {
+        // per-pixel statistics are per micrograph: one search each
+        for (int m = 0; m < n_micrographs; ++m) {
+            std::vector<MicPlan> one(1);
+            one[0].host = host_micrographs[m];
+            one[0].nx = nx[m];
+            one[0].ny = ny[m];
+            one[0].ctf = ctfs[m];
+            std::vector<std::vector<gs_pick>> r1;
+            TRY(search_many(ctx, one, &r1));
+            res[m] = std::move(r1[0]);
+        }
+    } else {
+        std::vector<MicPlan> mics(n_micrographs);
+        for (int m = 0; m < n_micrographs; ++m) {
+            mics[m].host = host_micrographs[m];
+            mics[m].nx = nx[m];
+            mics[m].ny = ny[m];
+            mics[m].ctf = ctfs[m];
+        }
+        TRY(search_many(ctx, mics, &res));
+    }
+    return hand_out(ctx, res, picks, n_picks, picks_per_micrograph);
 }
 
 int gs_get_units(gs_ctx* ctx, gs_unit* host_out, size_t cap, size_t* n_out) {
@@ -1054,8 +1370,20 @@ int gs_set_option(gs_ctx* ctx, int option, int value) {
             if (value < 1) return set_err(ctx, GS_ERR_ARG, "window block must be >= 1");
             ctx->window_block = value;
             return GS_OK;
+        case GS_OPT_CORR_CTAS:
+            if (value < 0) return set_err(ctx, GS_ERR_ARG, "CTAs per SM must be >= 0");
+            ctx->corr_ctas = value;
+            return GS_OK;
+        case GS_OPT_GRAPH: ctx->use_graph = value != 0; return GS_OK;
+        case GS_OPT_AUTOTUNE: ctx->autotune = value != 0; return GS_OK;
         default: return set_err(ctx, GS_ERR_ARG, "unknown option %d", option);
     }
+}
+
+int gs_get_tuning(gs_ctx* ctx, int* out4) {
+    if (!ctx || !out4) return set_err(ctx, GS_ERR_ARG, "null pointer");
+    for (int i = 0; i < 4; ++i) out4[i] = ctx->last_tuning[i];
+    return GS_OK;
 }
 
 int gs_set_kernel_timing(gs_ctx* ctx, int enable) {

@@ -616,15 +616,21 @@ struct PickDev {
 // Threshold + border test of every unit, compacted with an atomic counter
 // (order restored on the host by sorting on `unit`).  Reference:
 // main.cu:878-890.
+// Threshold + centre test of the units of one micrograph (main.cu:869-891).
+// The micrograph owns windows [w0, w0 + nw) of a units table laid out
+// [angle][NW windows][nt templates]; pick.unit is its local index
+// (angle, window, template), the reference's line order.
 __global__ void k_compact(const UnitOut* __restrict__ units, long long total, int nw, int nt, int bx,
                           const int* __restrict__ offx, const int* __restrict__ offy, int l, float d_m, int nx, int ny,
                           float thres, PickDev* __restrict__ picks, unsigned long long* __restrict__ count,
-                          long long cap) {
+                          long long cap, int NW, int w0) {
     const long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= total) return;
-    const UnitOut r = units[u];
+    const long long per = (long long)nw * nt;
+    const long long ai = u / per, rem = u - ai * per;
+    const UnitOut r = units[(ai * NW + w0) * nt + rem];
     if (!(r.score >= thres)) return;
-    const int w = (int)((u / nt) % nw);
+    const int w = (int)(rem / nt);
     const int i = w % bx, j = w / bx;
     const float cx = (float)(offx[i] + r.pos % l);
     const float cy = (float)(offy[j] + r.pos / l);

@@ -1,0 +1,361 @@
+// Persistent correlation kernel with the N2-point DFT stage on the tensor
+// cores (tcgen05, split 16-bit precision, f32 accumulation in TMEM).
+//
+// Same work queue, dependencies, scratch ring and bounded waits as
+// k_corr_persistent (corr.cuh); the tiles differ.  The length-L inverse DFT
+// of a vector (L = 16 N2) is taken in four steps with n = N2 a + b and
+// k = ka + 16 kb:
+//   1. for each b: 16-point DFT over a in FP32 registers (regfft.cuh), then
+//      the twiddle exp(+2 pi i b ka / L)            -> Y[v][ka][b]
+//   2. for each (v, ka): N2-point DFT over b as a real GEMM on the tensor
+//      cores: D[(v,ka)][(kb,c')] = sum_(b,c) Y[(v,ka)][(b,c)] F[(kb,c')][(b,c)]
+//      with F the real form of exp(+2 pi i b kb / N2).
+// Both Y and F are split into 16-bit (hi, lo) parts and D accumulates
+// hi*hi + lo*hi + hi*lo, so the stage keeps about 16 (BF16) or 22 (FP16)
+// significant bits per operand.  FP16 needs bounded data (see a_scale).
+//
+// A tile is 8 vectors (rows in the row pass, columns in the column pass):
+// the GEMM has M = 8 x 16 = 128 rows (row index ka * 8 + v), K = N = 2 N2
+// rounded up to 16.  One thread issues the MMAs; the CTA waits on an
+// mbarrier the MMAs' commit arrives on; every warp then reads its 32 TMEM
+// lanes.  128 threads per CTA, two CTAs per SM, so one CTA's MMAs overlap the
+// other's FP32 work.  Operands are K-major interleaved tiles (tc.cuh).
+#pragma once
+
+#include "corr.cuh"
+#include "tc.cuh"
+
+namespace gs {
+
+constexpr int kTcThreads = 128;
+constexpr int kTcWarps = kTcThreads / 32;
+
+template <int N2, bool kBf16>
+struct TcCfg {
+    static constexpr int L = 16 * N2;
+    static constexpr int V = 8;                         // vectors per tile
+    static constexpr int T = L / V;                     // tiles per pass of one unit
+    static constexpr int KP = ((2 * N2 + 15) / 16) * 16;  // GEMM K = N
+    static constexpr int M = 128;
+    static constexpr uint32_t idesc = tc::idesc_f16(M, KP, kBf16 ? 1 : 0);
+    // FP16 keeps the data operand inside its range (max 65504) by an exact
+    // power-of-two prescale, undone by the matrix: (A / 16) (16 F) = A F.
+    // With amplitude-normalised spectra (phase_flip 1) the data stays below
+    // about 2e4 at l <= 768.
+    static constexpr float a_scale = kBf16 ? 1.0f : 0.0625f;
+    static constexpr float b_scale = kBf16 ? 1.0f : 16.0f;
+    // shared memory
+    static constexpr size_t a_bytes = (size_t)M * KP * 2;   // one of hi / lo
+    static constexpr size_t b_bytes = (size_t)KP * KP * 2;
+    static constexpr size_t off_a_hi = 0;
+    static constexpr size_t off_a_lo = off_a_hi + a_bytes;
+    static constexpr size_t off_b_hi = off_a_lo + a_bytes;
+    static constexpr size_t off_b_lo = off_b_hi + b_bytes;
+    static constexpr size_t off_tw = off_b_lo + b_bytes;
+    static constexpr size_t off_bar = off_tw + (size_t)16 * N2 * sizeof(float2);
+    static constexpr size_t off_misc = off_bar + 16;      // tmem slot + 4 broadcast slots
+    static constexpr size_t bytes = off_misc + 32;
+    static constexpr uint32_t tmem_cols = KP <= 64 ? 64 : 128;
+    static_assert(L % V == 0, "tile");
+    static_assert(KP <= 256 && KP % 16 == 0, "N");
+};
+
+// Step 1 of a tile: FP32 16-point DFTs + twiddle, split and stored into the
+// A operand.  Lane mapping v = task % 8, b = task / 8 keeps both the global
+// loads (8 rows x 4 consecutive b, or 4 rows x 8 consecutive columns) and
+// the 4-byte shared stores (banks (v, b % 4)) conflict-free.
+template <int N2, bool kBf16, class Load>
+__device__ __forceinline__ void tc_step1(const Load& load, unsigned char* sm, const float2* twt) {
+    using C = TcCfg<N2, kBf16>;
+    unsigned char* a_hi = sm + C::off_a_hi;
+    unsigned char* a_lo = sm + C::off_a_lo;
+    for (int task = threadIdx.x; task < C::V * N2; task += kTcThreads) {
+        const int v = task & 7, b = task >> 3;
+        float2 x[16];
+#pragma unroll
+        for (int a = 0; a < 16; ++a) x[a] = load(v, N2 * a + b);
+        rf::rfft<16, 1, true>(x);
+        rf::static_for<16>([&](auto kc) {
+            constexpr int ka = decltype(kc)::value;
+            float2 y = ka ? cmul(x[rf::rpos<16>(ka)], twt[ka * N2 + b]) : x[rf::rpos<16>(ka)];
+            if (!kBf16) y = cscale(y, C::a_scale);
+            uint32_t hi, lo;
+            tc::Split<kBf16>::run(y.x, y.y, hi, lo);
+            const uint32_t off = tc::kmajor_off(ka * 8 + v, 2 * b, C::M);
+            *reinterpret_cast<uint32_t*>(a_hi + off) = hi;
+            *reinterpret_cast<uint32_t*>(a_lo + off) = lo;
+        });
+    }
+}
+
+// Step 2: the split GEMM, issued by thread 0, completion on the mbarrier.
+template <int N2, bool kBf16>
+__device__ __forceinline__ void tc_issue(unsigned char* sm, uint32_t tmem, uint64_t* bar) {
+    using C = TcCfg<N2, kBf16>;
+    if (threadIdx.x != 0) return;
+    const uint32_t a_hi = tc::smem_u32(sm + C::off_a_hi), a_lo = tc::smem_u32(sm + C::off_a_lo);
+    const uint32_t b_hi = tc::smem_u32(sm + C::off_b_hi), b_lo = tc::smem_u32(sm + C::off_b_lo);
+    constexpr uint32_t lbo_a = C::M * 16, lbo_b = C::KP * 16;
+    uint32_t acc = 0;
+#pragma unroll
+    for (int j = 0; j < C::KP / 16; ++j) {
+        const uint32_t oa = 2 * j * lbo_a, ob = 2 * j * lbo_b;
+        tc::mma_f16(tmem, tc::smem_desc(a_hi + oa, lbo_a, 128), tc::smem_desc(b_hi + ob, lbo_b, 128), C::idesc, acc);
+        acc = 1;
+        tc::mma_f16(tmem, tc::smem_desc(a_lo + oa, lbo_a, 128), tc::smem_desc(b_hi + ob, lbo_b, 128), C::idesc, 1);
+        tc::mma_f16(tmem, tc::smem_desc(a_hi + oa, lbo_a, 128), tc::smem_desc(b_lo + ob, lbo_b, 128), C::idesc, 1);
+    }
+    tc::mma_commit(bar);
+}
+
+// Publish step 1 to the tensor core, run step 2, wait for it.  Returns false
+// when the bounded wait gave up (the error flag is raised by the caller).
+template <int N2, bool kBf16>
+__device__ __forceinline__ bool tc_gemm(unsigned char* sm, uint32_t tmem, uint64_t* bar, uint32_t& phase) {
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    tc_issue<N2, kBf16>(sm, tmem, bar);
+    __syncwarp();
+    const bool ok = tc::mbar_wait(bar, phase, 1u << 24);
+    phase ^= 1u;
+    tc::fence_after_sync();
+    return ok;
+}
+
+// Reads 8 complex outputs (kb = 8 q .. 8 q + 7) of this thread's GEMM row.
+__device__ __forceinline__ void tc_read8(uint32_t tmem, int q, float2* out) {
+    float f[16];
+    tc::tmem_ld16(tmem + ((uint32_t)(32 * (threadIdx.x >> 5)) << 16) + (uint32_t)(16 * q), f);
+    tc::tmem_ld_wait();
+#pragma unroll
+    for (int i = 0; i < 8; ++i) out[i] = make_float2(f[2 * i], f[2 * i + 1]);
+}
+
+template <int N2, bool kBf16>
+__device__ __forceinline__ bool tc_row_tile(const CorrArgs& a, int u, int t, unsigned char* sm, const float2* twt,
+                                            uint32_t tmem, uint64_t* bar, uint32_t& phase) {
+    using C = TcCfg<N2, kBf16>;
+    constexpr int L = C::L;
+    const int2 wp = a.unit_wp[u];
+    const float2* Wr = a.W + (long long)wp.x * a.L2;
+    const float2* Pr = a.P + (long long)wp.y * a.L2;
+    float2* Rs = a.R + (long long)(u % a.S) * a.L2;
+    const int r0 = t * C::V;
+    const unsigned long long keep = l2_policy_evict_last();
+    auto load = [&](int v, int n) {
+        const long long o = (long long)(r0 + v) * L + n;
+        return cmulc(ld_l2hint(Wr + o, keep), __ldg(Pr + o));
+    };
+    tc_step1<N2, kBf16>(load, sm, twt);
+    const bool ok = tc_gemm<N2, kBf16>(sm, tmem, bar, phase);
+    const int r = threadIdx.x, ka = r >> 3, v = r & 7;
+    float2* dst = Rs + (long long)(r0 + v) * L + ka;
+#pragma unroll 1
+    for (int q = 0; q < (N2 + 7) / 8; ++q) {
+        float2 o[8];
+        tc_read8(tmem, q, o);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int kb = 8 * q + i;
+            if (kb < N2) st_l2hint(dst + 16 * kb, o[i], keep);
+        }
+    }
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) {
+        __threadfence();
+        atomicAdd(&a.done_rows[u], 1);
+    }
+    return ok;
+}
+
+template <int N2, bool kBf16>
+__device__ __forceinline__ bool tc_col_tile(const CorrArgs& a, int u, int t, unsigned char* sm, const float2* twt,
+                                            uint32_t tmem, uint64_t* bar, uint32_t& phase, bool* last_out) {
+    using C = TcCfg<N2, kBf16>;
+    constexpr int L = C::L;
+    constexpr int h = L / 2;
+    const float2* Rs = a.R + (long long)(u % a.S) * a.L2;
+    const int c0 = t * C::V;
+    const unsigned long long drop = l2_policy_evict_first();
+    auto load = [&](int v, int n) { return ld_l2hint(Rs + (long long)n * L + c0 + v, drop); };
+    tc_step1<N2, kBf16>(load, sm, twt);
+    const bool ok = tc_gemm<N2, kBf16>(sm, tmem, bar, phase);
+    const int r = threadIdx.x, ka = r >> 3, v = r & 7;
+    const int x = c0 + v;
+    const bool xin = (unsigned)(x - a.yb0) > (unsigned)(a.yb1 - a.yb0);
+    float best1 = 0.0f, best2 = 0.0f;
+    int bk1 = -1, bk2 = -1;
+    float s1a = 0.f, s2a = 0.f, s1b = 0.f, s2b = 0.f;
+#pragma unroll 1
+    for (int q = 0; q < (N2 + 7) / 8; ++q) {
+        float2 o[8];
+        tc_read8(tmem, q, o);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int kb = 8 * q + i;
+            if (kb >= N2) break;
+            const int y = ka + 16 * kb;
+            const bool in = xin && ((unsigned)(y - a.yb0) > (unsigned)(a.yb1 - a.yb0));
+            const float v1 = ((L / 2) % 2 == 0) ? o[i].x : -o[i].x;
+            const float v2 = ((L / 2) % 2 == 0) ? o[i].y : -o[i].y;
+            const bool g1 = in && v1 > best1, g2 = in && v2 > best2;
+            best1 = g1 ? v1 : best1;
+            bk1 = g1 ? kb : bk1;
+            best2 = g2 ? v2 : best2;
+            bk2 = g2 ? kb : bk2;
+            s1a += v1; s2a = fmaf(v1, v1, s2a);
+            s1b += v2; s2b = fmaf(v2, v2, s2b);
+        }
+    }
+    const int X = x + h < L ? x + h : x - h;
+    unsigned long long ka_key = 0ull, kb_key = 0ull;
+    if (bk1 >= 0) {
+        const int y = ka + 16 * bk1;
+        const int Y = y + h < L ? y + h : y - h;
+        ka_key = argmax_key(best1, Y * L + X);
+    }
+    if (bk2 >= 0) {
+        const int y = ka + 16 * bk2;
+        const int Y = y + h < L ? y + h : y - h;
+        kb_key = argmax_key(best2, Y * L + X);
+    }
+    double d1a = warp_sum((double)s1a), d2a = warp_sum((double)s2a);
+    double d1b = warp_sum((double)s1b), d2b = warp_sum((double)s2b);
+    ka_key = warp_max_u64(ka_key);
+    kb_key = warp_max_u64(kb_key);
+    bool last = false;
+    if ((threadIdx.x & 31) == 0) {
+        UnitAcc* ac = a.acc + 2 * (long long)u;
+        if (ka_key) atomicMax(&ac[0].key, ka_key);
+        atomicAdd(&ac[0].s1, d1a);
+        atomicAdd(&ac[0].s2, d2a);
+        if (kb_key) atomicMax(&ac[1].key, kb_key);
+        atomicAdd(&ac[1].s1, d1b);
+        atomicAdd(&ac[1].s2, d2b);
+        __threadfence();
+        last = atomicAdd(&a.done_cols[u], 1) == kTcWarps * C::T - 1;
+    }
+    *last_out = last;
+    return ok;
+}
+
+template <int N2, bool kBf16>
+__device__ __forceinline__ void tc_wait_for(const CorrArgs& a, int item) {
+    using C = TcCfg<N2, kBf16>;
+    const int s = item / (2 * C::T), j = item - s * (2 * C::T);
+    if (j < C::T) {
+        if (s < a.nu && s >= a.S) wait_counter(a.done_cols + (s - a.S), kTcWarps * C::T, a.error);
+    } else {
+        const int u = s - a.lag;
+        if (u >= 0 && u < a.nu) wait_counter(a.done_rows + u, kTcWarps * C::T, a.error);
+    }
+}
+
+template <int N2, bool kBf16>
+__global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(CorrArgs a) {
+    using C = TcCfg<N2, kBf16>;
+    extern __shared__ __align__(128) unsigned char smt[];
+    float2* twt = reinterpret_cast<float2*>(smt + C::off_tw);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smt + C::off_bar);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smt + C::off_misc);
+    int* ish = reinterpret_cast<int*>(smt + C::off_misc + 16);
+    // twiddles exp(+2 pi i b ka / L), table [ka][b]
+    for (int i = threadIdx.x; i < 16 * N2; i += kTcThreads) {
+        const int ka = i / N2, b = i - ka * N2;
+        double sn, cs;
+        sincospi(2.0 * (double)((b * ka) % C::L) / (double)C::L, &sn, &cs);
+        twt[i] = make_float2((float)cs, (float)sn);
+    }
+    // DFT-N2 matrix (inverse sign), real form, split; rows (kb, c'), columns (b, c)
+    for (int i = threadIdx.x; i < C::KP * C::KP / 2; i += kTcThreads) {
+        const int row = (2 * i) / C::KP, col = (2 * i) % C::KP;  // col even: (b, re), (b, im)
+        const int kb = row >> 1, cp = row & 1, b = col >> 1;
+        float e0 = 0.f, e1 = 0.f;
+        if (kb < N2 && b < N2) {
+            double sn, cs;
+            sincospi(2.0 * (double)((b * kb) % N2) / (double)N2, &sn, &cs);
+            // out_re = x_re cos - x_im sin ; out_im = x_re sin + x_im cos
+            e0 = cp ? (float)sn : (float)cs;
+            e1 = cp ? (float)cs : (float)-sn;
+        }
+        e0 *= C::b_scale;
+        e1 *= C::b_scale;
+        uint32_t hi, lo;
+        tc::Split<kBf16>::run(e0, e1, hi, lo);
+        const uint32_t off = tc::kmajor_off(row, col, C::KP);
+        *reinterpret_cast<uint32_t*>(smt + C::off_b_hi + off) = hi;
+        *reinterpret_cast<uint32_t*>(smt + C::off_b_lo + off) = lo;
+    }
+    // K padding of the A operand stays zero (step 1 writes only b < N2)
+    for (int i = threadIdx.x; i < C::M * C::KP / 2; i += kTcThreads) {
+        const int row = (2 * i) / C::KP, col = (2 * i) % C::KP;
+        if ((col >> 1) >= N2) {
+            const uint32_t off = tc::kmajor_off(row, col, C::M);
+            *reinterpret_cast<uint32_t*>(smt + C::off_a_hi + off) = 0u;
+            *reinterpret_cast<uint32_t*>(smt + C::off_a_lo + off) = 0u;
+        }
+    }
+    if ((threadIdx.x >> 5) == 0) tc::tmem_alloc(tslot, C::tmem_cols);
+    if (threadIdx.x == 0) {
+        tc::mbar_init(bar, 1);
+        tc::fence_mbar_init();
+    }
+    const int total = (a.nu + a.lag) * 2 * C::T;
+    if (threadIdx.x == 0) {
+        const int first = atomicAdd(a.next_item, 1);
+        if (first < total) tc_wait_for<N2, kBf16>(a, first);
+        ish[0] = first;
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *tslot;
+    uint32_t phase = 0;
+    bool ok = true;
+    int item = ish[0];
+    for (int iter = 1; item < total; ++iter) {
+        int nxt = 0;
+        if (threadIdx.x == 0) nxt = atomicAdd(a.next_item, 1);
+        const int s = item / (2 * C::T), j = item - s * (2 * C::T);
+        if (j < C::T) {
+            if (s < a.nu) ok &= tc_row_tile<N2, kBf16>(a, s, j, smt, twt, tmem, bar, phase);
+        } else {
+            const int u = s - a.lag;
+            if (u >= 0 && u < a.nu) {
+                bool last = false;
+                ok &= tc_col_tile<N2, kBf16>(a, u, j - C::T, smt, twt, tmem, bar, phase, &last);
+                if ((threadIdx.x & 31) == 0 && last) {
+                    __threadfence();
+                    const int2 wp = a.unit_wp[u];
+                    const UnitAcc* ac = a.acc + 2 * (long long)u;
+                    for (int q = 0; q < 2; ++q) {
+                        const int J = 2 * wp.y + q;
+                        if (J >= a.ntmpl) break;
+                        UnitAcc v;
+                        v.key = __ldcg(&ac[q].key);
+                        v.s1 = __ldcg(&ac[q].s1);
+                        v.s2 = __ldcg(&ac[q].s2);
+                        a.out[(long long)wp.x * a.ntmpl + J] = unit_score(v, C::L);
+                    }
+                }
+            }
+        }
+        if (threadIdx.x == 0) {
+            if (nxt < total) tc_wait_for<N2, kBf16>(a, nxt);
+            ish[iter & 3] = nxt;
+        }
+        // the A operand and TMEM are free again (all reads done) and the next
+        // item is published
+        tc::fence_before_sync();
+        __syncthreads();
+        tc::fence_after_sync();
+        item = ish[iter & 3];
+    }
+    if (!ok && threadIdx.x == 0) atomicExch(a.error, 1);
+    __syncthreads();
+    if ((threadIdx.x >> 5) == 0) tc::tmem_dealloc(tmem, C::tmem_cols);
+}
+
+}  // namespace gs

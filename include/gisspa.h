@@ -61,10 +61,22 @@ typedef struct gs_params {
     float ampconst;    /* amplitude contrast (fixed 0.07 in the reference) */
     float a, b, b2;    /* noise-curve constants (DataReader.h:25) */
     float bfactor, bfactor2, bfactor3; /* signal-curve constants */
-    int precision;     /* GS_PREC_FP32 (the only mode in this build) */
+    int precision;     /* arithmetic of the correlation's DFT stages (no
+                          reference counterpart; default GS_PREC_FP32) */
 } gs_params;
 
+/* GS_PREC_FP32: every FFT stage in FP32 on the CUDA cores (the reference's
+ * precision).  GS_PREC_TC_BF16 / GS_PREC_TC_FP16: the N2-point DFT stage of
+ * the correlation (window l = 16 * N2 with N2 = 32, 45 or 48, persistent
+ * path) runs on the tensor cores as a GEMM with operands split into 16-bit
+ * (hi, lo) parts, hi*hi + lo*hi + hi*lo accumulated in FP32; other stages
+ * stay FP32.  Other windows, the two-pass path and norm_type 1 return
+ * GS_ERR_UNSUPPORTED with these modes; GS_PREC_TC_FP16 also needs
+ * phase_flip 1 (its data operand relies on amplitude-normalised spectra to
+ * stay inside the FP16 range). */
 #define GS_PREC_FP32 0
+#define GS_PREC_TC_BF16 1
+#define GS_PREC_TC_FP16 2
 
 /* Per-micrograph CTF line values as in the input list
  * (DataReader.cpp:366-388: defocus=, dfdiff=, dfang=). */
@@ -142,6 +154,21 @@ int gs_get_geometry(struct gs_ctx* ctx, int nx, int ny, gs_geometry* out);
 int gs_search(struct gs_ctx* ctx, const float* host_micrograph, int nx, int ny,
               const gs_ctf* ctf, gs_pick** picks, size_t* n_picks);
 
+/* Several micrographs, possibly of different sizes, in one search with the
+ * loaded templates (no reference counterpart: the reference loops over its
+ * input list, main.cu:1149-1269, and re-does every angle's template spectra
+ * per micrograph).  All micrographs' windows share the window-spectrum array
+ * and each angle's template spectra; the persistent correlation runs over
+ * every (window, template pair) of the batch in one launch per angle.  Picks
+ * equal those of one gs_search per micrograph; they come back concatenated in
+ * micrograph order, picks_per_micrograph[m] (caller array of n_micrographs)
+ * telling how many belong to each.  host_micrographs[m]: ny[m] x nx[m]
+ * float32 row-major; ctfs[m] its CTF line.  With norm_type 1 the micrographs
+ * are searched one after the other. */
+int gs_search_batch(struct gs_ctx* ctx, int n_micrographs, const float* const* host_micrographs,
+                    const int* nx, const int* ny, const gs_ctf* ctfs, gs_pick** picks, size_t* n_picks,
+                    size_t* picks_per_micrograph);
+
 /* Same search with the micrograph already in device memory (ny x nx float32
  * on the context's device).  The micrograph is not modified. */
 int gs_search_device(struct gs_ctx* ctx, const float* device_micrograph, int nx, int ny,
@@ -167,6 +194,11 @@ void gs_picks_free(gs_pick* picks);
 #define GS_TIMING_COUNT 8
 int gs_get_timings(struct gs_ctx* ctx, float* out, int n);
 
+/* Scheduling the last search used for the persistent correlation (after
+ * autotuning when GS_OPT_AUTOTUNE is on): out4 = {ring slots, lag, window
+ * block, CTAs per SM (0 = as many as fit)}. */
+int gs_get_tuning(struct gs_ctx* ctx, int* out4);
+
 /* Enable (1) or disable (0) per-kernel event timing of the correlation
  * passes; it adds two events per launch. */
 int gs_set_kernel_timing(struct gs_ctx* ctx, int enable);
@@ -187,6 +219,19 @@ int gs_set_kernel_timing(struct gs_ctx* ctx, int enable);
  * column tiles are queued (default 6); slots must exceed lag. */
 #define GS_OPT_CORR_SLOTS 4
 #define GS_OPT_CORR_LAG 5
+/* GS_OPT_CORR_CTAS: resident CTAs per SM of the persistent launch (0 = as
+ * many as shared memory, registers and TMEM allow; default 0). */
+#define GS_OPT_CORR_CTAS 6
+/* GS_OPT_GRAPH: 1 = capture the whole angle loop (template spectra +
+ * correlation of every angle) as one CUDA graph and launch it once; per-angle
+ * timings are then not available (gs_get_timings [1] is 0 and [2] holds the
+ * graph's time). */
+#define GS_OPT_GRAPH 7
+/* GS_OPT_AUTOTUNE: 1 = before the first search of a given (window,
+ * templates, windows, precision), time candidate ring slots, lag, window
+ * block and CTAs per SM on angle 0 over up to 8192 units and keep the
+ * fastest for this context (gs_get_tuning shows the choice). */
+#define GS_OPT_AUTOTUNE 8
 int gs_set_option(struct gs_ctx* ctx, int option, int value);
 
 /* Counters of this context since creation (no reference counterpart; the
