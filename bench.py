@@ -232,6 +232,106 @@ DTYPES = {"fp32": "f32", "tc-bf16": "bf16 hi+lo split, f32 accumulate",
           "tc-fp16": "fp16 hi+lo split, f32 accumulate"}
 
 
+def tensor_core_comparison(ds, kw, local_rank, base_precision: str):
+    """The two correlation paths on the same micrograph and templates over
+    three in-plane angles (0, 120, 240 deg): per-angle correlation time of
+    the FP32 path and the tensor-core path (split BF16), their ratio, the
+    per-micrograph rate each implies at 72 angles, and whether their picks
+    are equal (same units, scores within 1e-4)."""
+    import numpy as np
+    import gisspa_b200 as G
+    m = ds.micrographs[0]
+    ctf = (m.defocus, m.dfdiff, m.dfang)
+    res, picks = {}, {}
+    for name in ("fp32", "tc-bf16"):
+        params = params_for(ds, kw)
+        params.phi_step = 120.0
+        params.precision = PRECISION_MODES[name]
+        with G.Context(local_rank) as ctx:
+            ctx.set_templates(params, ds.templates, ctf)
+            ctx.search(m.image, ctf)                       # warm-up
+            corr, prep_spec = [], []
+            for _ in range(2):
+                pk = ctx.search(m.image, ctf)
+                t = ctx.timings()
+                corr.append(t[2] / 3.0)
+                prep_spec.append(t[0] + t[1] / 3.0)
+            picks[name] = pk
+            res[name] = {"per_angle_correlation_ms": float(np.mean(corr)),
+                         "micrograph_prep_plus_spectra_per_angle_ms": float(np.mean(prep_spec))}
+    a, b = picks["fp32"], picks["tc-bf16"]
+    key = lambda p: (int(p["angle_index"]), int(p["window_x"]), int(p["window_y"]),
+                     int(p["template_index"]), float(p["center_x"]), float(p["center_y"]))
+    ka, kb = {key(p): float(p["score"]) for p in a}, {key(p): float(p["score"]) for p in b}
+    common = set(ka) & set(kb)
+    rel = max([abs(ka[k] - kb[k]) / abs(ka[k]) for k in common], default=0.0)
+    out = {"angles_timed": 3, "note": "same micrograph and templates as the headline; per-angle times "
+           "extrapolated to 72 angles for the micrographs/s of each path",
+           "fp32": res["fp32"], "tc_bf16": res["tc-bf16"],
+           "tc_over_fp32_speed": res["fp32"]["per_angle_correlation_ms"] / res["tc-bf16"]["per_angle_correlation_ms"],
+           "equal_picks": set(ka) == set(kb) and rel <= 1e-4, "picks": [len(a), len(b)],
+           "max_rel_score_diff": rel}
+    for name, r in (("fp32", res["fp32"]), ("tc_bf16", res["tc-bf16"])):
+        ms = r["micrograph_prep_plus_spectra_per_angle_ms"] + 72 * r["per_angle_correlation_ms"]
+        out[name]["micrographs_per_s_at_72_angles"] = 1000.0 / ms
+    return out
+
+
+def refinement_report(ctx, geom, m, n_picks=2048, steps=20, n_judge=256):
+    """Off-grid refinement of the search's best units (gs_refine) on the
+    headline micrograph: time, share of picks whose score rises over the grid
+    score, and a judge: for n_judge picks the best score of a dense local grid
+    (angle +-1 deg in 0.5 deg, shift +-0.5 px in 0.25 px, defocus +-100 A in
+    50 A; 625 points, evaluated through gs_score_grad) against the refined
+    score."""
+    import numpy as np
+    import gisspa_b200 as G
+    na, nw, nt = geom.n_angles, geom.n_windows_x * geom.n_windows_y, geom.n_templates
+    u = ctx.units((na, nw, nt))
+    sc = np.where(np.isfinite(u["score"]), u["score"], -np.inf)
+    order = np.argsort(sc, axis=None)[::-1][:n_picks]
+    step = 360.0 / na
+    pk = np.zeros(len(order), dtype=G.REFINE_PICK_DTYPE)
+    for q, flat in enumerate(order):
+        ai, w, J = np.unravel_index(flat, sc.shape)
+        pk[q] = (w, J, int(u["pos"][ai, w, J]), ai * step, 0.0, 0.0, m.defocus, m.dfdiff, m.dfang)
+    t0 = time.perf_counter()
+    start = ctx.score_grad(pk, with_gradient=False)["score"]
+    t1 = time.perf_counter()
+    refined, res = ctx.refine(pk, steps=steps)
+    t2 = time.perf_counter()
+    gain = res["score"] - start
+    out = {"picks": int(len(pk)), "steps": steps, "refine_s": t2 - t1, "score_s": t1 - t0,
+           "improved_frac": float((gain > 1e-6 * np.abs(start)).mean()),
+           "lowered": int((gain < -1e-6 * np.abs(start)).sum()),
+           "median_gain": float(np.median(gain)), "median_grid_score": float(np.median(start))}
+    nj = min(n_judge, len(pk))
+    offs_a = np.arange(-2, 3) * 0.5
+    offs_d = np.arange(-2, 3) * 0.25
+    offs_f = np.arange(-2, 3) * 0.005
+    grid = []
+    for q in range(nj):
+        for da in offs_a:
+            for ddx in offs_d:
+                for ddy in offs_d:
+                    for df in offs_f:
+                        p = pk[q].copy()
+                        p["angle"] += da
+                        p["dx"], p["dy"] = ddx, ddy
+                        p["defocus"] += df
+                        grid.append(p)
+    grid = np.array(grid, dtype=G.REFINE_PICK_DTYPE)
+    t3 = time.perf_counter()
+    gs = ctx.score_grad(grid, with_gradient=False)["score"].reshape(nj, -1)
+    t4 = time.perf_counter()
+    best = gs.max(axis=1)
+    out["judge"] = {"picks": nj, "grid": "5 angles (0.5 deg) x 5 x 5 shifts (0.25 px) x 5 defocus (50 A)",
+                    "grid_s": t4 - t3,
+                    "refined_ge_grid_best_frac": float((res["score"][:nj] >= best - 1e-4 * np.abs(best)).mean()),
+                    "median_refined_minus_grid_best": float(np.median(res["score"][:nj] - best))}
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import gisspa_b200 as G
@@ -319,7 +419,9 @@ def run_ours(args, rank, world, local_rank):
         achieved = flops_launch / (avg_ms * 1e-3) / 1e12
         wblk = 4
         hbm_bytes = (npairs * math.ceil(nw / wblk) + nw) * l2 * 8.0   # P once per window block, W once
-        roof = {"bound": "fp32", "kernel": "k_corr_persistent (row + column tiles of one angle)",
+        kname = ("k_corr_persistent (row + column tiles of one angle)" if args.precision == "fp32" else
+                 "k_corr_tc (row + column tiles of one angle; N2-point DFT stage on the tensor cores)")
+        roof = {"bound": "fp32", "kernel": kname,
                 "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
                 "traffic": None, "peak_source": "148 SMs x 256 FLOP/clk x median SM clock under load",
                 "algorithmic_flops_per_launch": flops_launch, "avg_launch_ms": avg_ms, "launches": kn,
@@ -370,6 +472,17 @@ def run_ours(args, rank, world, local_rank):
                      "correlation": float(t[2])},
         "clocks": clocks,
     }
+    if world == 1 and not args.no_refine and not args.templates:
+        try:
+            # the context still holds the units of the last timed search
+            line["refinement"] = refinement_report(ctx, geom, m)
+        except Exception as e:  # reported, not fatal
+            line["refinement"] = {"error": repr(e)}
+    if world == 1 and not args.no_tc_compare and args.workload == "full" and not args.templates:
+        try:
+            line["tensor_core"] = tensor_core_comparison(ds, kw, local_rank, args.precision)
+        except Exception as e:  # reported, not fatal
+            line["tensor_core"] = {"error": repr(e)}
     if world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(ds, kw, geom)
@@ -455,6 +568,9 @@ def main() -> int:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["full", "small"], default="full")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-refine", action="store_true", help="skip the off-grid refinement report")
+    ap.add_argument("--no-tc-compare", action="store_true",
+                    help="skip the FP32 vs tensor-core comparison over three angles")
     ap.add_argument("--precision", choices=sorted(PRECISION_MODES), default="fp32",
                     help="arithmetic of the correlation's N2-point DFT stage")
     # profiling aids (smaller captures); a line produced with them names the reduced workload

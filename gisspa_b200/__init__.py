@@ -60,6 +60,11 @@ class GsStats(C.Structure):
                 ("units", C.c_ulonglong)]
 
 
+REFINE_PICK_DTYPE = np.dtype([("window", "<i4"), ("template_index", "<i4"), ("pos", "<i4"),
+                              ("angle", "<f4"), ("dx", "<f4"), ("dy", "<f4"), ("defocus", "<f4"),
+                              ("dfdiff", "<f4"), ("dfang", "<f4")])
+REFINE_RESULT_DTYPE = np.dtype([("score", "<f4"), ("d_angle", "<f4"), ("d_dx", "<f4"), ("d_dy", "<f4"),
+                                ("d_defocus", "<f4"), ("d_dfdiff", "<f4"), ("d_dfang", "<f4")])
 UNIT_DTYPE = np.dtype([("score", "<f4"), ("pos", "<i4"), ("peak", "<f4"), ("sigma", "<f4")])
 PICK_DTYPE = np.dtype([("angle_index", "<i4"), ("phi", "<f4"), ("window_x", "<i4"),
                        ("window_y", "<i4"), ("template_index", "<i4"), ("center_x", "<f4"),
@@ -70,7 +75,8 @@ EXPORTS = ("gs_status_string", "gs_version", "gs_params_default", "gs_ctx_create
            "gs_ctx_destroy", "gs_ctx_last_error", "gs_set_templates", "gs_get_geometry",
            "gs_search", "gs_search_device", "gs_get_units", "gs_picks_free", "gs_get_timings",
            "gs_get_stats", "gs_set_kernel_timing", "gs_set_option",
-           "gs_correlate_window_noalloc", "gs_search_batch", "gs_get_tuning")
+           "gs_correlate_window_noalloc", "gs_search_batch", "gs_get_tuning", "gs_score_grad",
+           "gs_refine")
 
 _lib_handle = None
 
@@ -120,6 +126,8 @@ def load_library(path: Optional[str] = None) -> C.CDLL:
                                     C.POINTER(C.POINTER(GsPick)), C.POINTER(C.c_size_t),
                                     C.POINTER(C.c_size_t)]
     lib.gs_get_tuning.argtypes = [vp, C.POINTER(C.c_int)]
+    lib.gs_score_grad.argtypes = [vp, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+    lib.gs_refine.argtypes = [vp, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
     if path is None:
         _lib_handle = lib
     return lib
@@ -238,6 +246,35 @@ class Context:
             out.append(allp[k:k + per[m]].copy())
             k += per[m]
         return out
+
+    def score_grad(self, picks: np.ndarray, with_gradient: bool = True,
+                   template_gradients: bool = False):
+        """gs_score_grad: objective (and gradient) of REFINE_PICK_DTYPE picks;
+        returns REFINE_RESULT_DTYPE results (and, with template_gradients,
+        d score / d template base as (n, l, l) float32)."""
+        pk = np.ascontiguousarray(picks, dtype=REFINE_PICK_DTYPE)
+        n = pk.shape[0]
+        out = np.zeros(n, dtype=REFINE_RESULT_DTYPE)
+        tg = None
+        if template_gradients and with_gradient and n:
+            l = self._l()
+            tg = np.zeros((n, l, l), dtype=np.float32)
+        self._check(self._lib.gs_score_grad(self._h, pk.ctypes.data, n, 1 if with_gradient else 0,
+                                            out.ctypes.data, tg.ctypes.data if tg is not None else None),
+                    "gs_score_grad")
+        return (out, tg) if template_gradients else out
+
+    def refine(self, picks: np.ndarray, steps: int = 20):
+        """gs_refine: gradient ascent; returns (refined picks, final results)."""
+        pk = np.array(picks, dtype=REFINE_PICK_DTYPE, copy=True)
+        out = np.zeros(pk.shape[0], dtype=REFINE_RESULT_DTYPE)
+        self._check(self._lib.gs_refine(self._h, pk.ctypes.data, pk.shape[0], int(steps), out.ctypes.data),
+                    "gs_refine")
+        return pk, out
+
+    def _l(self) -> int:
+        g = self.geometry(4096, 4096)
+        return int(g.l)
 
     def set_graph(self, enable: bool) -> None:
         """Capture the angle loop as one CUDA graph (GS_OPT_GRAPH)."""

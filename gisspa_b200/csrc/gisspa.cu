@@ -11,6 +11,7 @@
 #include "kernels.cuh"
 #include "norm1.cuh"
 #include "tccorr.cuh"
+#include "refine.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -57,6 +58,7 @@ struct gs_ctx {
     gs_ctf ctf0{};
     int l = 0, ntmpl = 0, tx = 0, ty = 0;
     DBuf tmpl;  // ntmpl x l x l float (real templates after preprocessing)
+    DBuf tbase; // ntmpl x l x l float (whitened templates before the CTF weight)
     // per-search buffers
     DBuf in, q, cimg, img, stats, ra, rb, off, win, wsum, winv;
     DBuf tspec, scratch, pstats, coef, acc, units, picks, count;
@@ -77,6 +79,8 @@ struct gs_ctx {
     int last_tuning[4] = {0, 0, 0, 0};
     unsigned long long graph_kernel_launches = 0;
     DBuf unit_wp, dep_counters, pacc, flags;
+    // off-grid refinement (refine.cuh): per-pick chunk buffers
+    DBuf rf_pk, rf_acc, rf_B, rf_F1, rf_T, rf_TM, rf_F, rf_G, rf_TB, rf_mask;
     std::vector<cudaEvent_t> kev;  // pool of events for per-kernel timing
     gs_stats counters{0, 0, 0};
 };
@@ -266,8 +270,14 @@ int launch_corr_tc_n2(gs_ctx* ctx, const CorrArgs& a, long long total_items) {
     int per_sm = 0, nsm = 0, dev = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTcThreads, C::bytes));
     if (per_sm < 1) return set_err(ctx, GS_ERR_UNSUPPORTED, "tensor-core kernel does not fit on an SM");
+    // Two CTAs per SM fit (2 x 93 KB of shared memory, 2 x 128 TMEM columns)
+    // even where the occupancy query reports one.  Launching CTAs that cannot
+    // be resident is harmless here: a CTA claims work items only while it
+    // runs, so no resident CTA ever waits on one that has not started.
+    per_sm = std::max(per_sm, 2);
     // TMEM: every resident CTA holds tmem_cols of the SM's 512 columns
     per_sm = std::min(per_sm, (int)(512 / C::tmem_cols));
     if (ctx->corr_ctas_override > 0) per_sm = std::min(per_sm, ctx->corr_ctas_override);
@@ -511,6 +521,243 @@ static int search_norm1(gs_ctx* ctx, const float2* W, int nx, int ny, const std:
     return GS_OK;
 }
 
+// Soft mask factor of apply_mask (GPU_func.cu:229-247), the arithmetic of
+// k_pair_rotate.
+__global__ void k_ref_mask(float* __restrict__ mask, int l, float d_m) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= l * l) return;
+    const int h = l / 2;
+    const int i = q % l, j = q / l;
+    const float dm = 1.5f * d_m;
+    const float rin = dm / 2.0f, rout = dm / 2.0f + 12.0f;
+    const float r = hypotf((float)(i - h), (float)(j - h));
+    float m = 1.0f;
+    if (r > rout) m = 0.0f;
+    else if (r >= rin) m = (float)(0.5 * (double)cosf((float)(kPiRef * (double)(r - rin) / 12.0)) + 0.5);
+    mask[q] = m;
+}
+
+// Objective (and with grad, its gradient) of n picks, chunked.  tgrad: host
+// n x l x l floats or null.
+static int score_grad_impl(gs_ctx* ctx, const gs_refine_pick* picks, int n, bool grad, gs_refine_result* out,
+                           float* tgrad) {
+    const gs_params& p = ctx->p;
+    const int l = ctx->l;
+    const long long l2 = (long long)l * l;
+    if (!ctx->have_units || ctx->last_nw <= 0)
+        return set_err(ctx, GS_ERR_STATE, "the window spectra of a norm_type 0 search are needed (search first)");
+    for (int i = 0; i < n; ++i) {
+        const gs_refine_pick& q = picks[i];
+        if (q.window < 0 || q.window >= ctx->last_nw || q.template_index < 0 || q.template_index >= ctx->ntmpl ||
+            q.pos < 0 || (long long)q.pos >= l2)
+            return set_err(ctx, GS_ERR_ARG, "pick %d: window, template or position out of range", i);
+        if (!std::isfinite(q.angle) || !std::isfinite(q.dx) || !std::isfinite(q.dy) || !std::isfinite(q.defocus) ||
+            !std::isfinite(q.dfdiff) || !std::isfinite(q.dfang))
+            return set_err(ctx, GS_ERR_ARG, "pick %d: parameter not finite", i);
+    }
+    // per-pick bytes: 6 complex + 2 real maps
+    const long long per = l2 * (6 * (long long)sizeof(float2) + 2 * (long long)sizeof(float));
+    const int chunk = (int)std::max<long long>(1, std::min<long long>(n, (2ll << 30) / per));
+    TRY(ensure(ctx, ctx->rf_pk, sizeof(RefinePickDev) * chunk));
+    TRY(ensure(ctx, ctx->rf_acc, sizeof(RefineAcc) * chunk));
+    TRY(ensure(ctx, ctx->rf_B, sizeof(float2) * l2 * chunk));
+    TRY(ensure(ctx, ctx->rf_F1, sizeof(float2) * l2 * chunk));
+    TRY(ensure(ctx, ctx->rf_T, sizeof(float2) * l2 * chunk));
+    TRY(ensure(ctx, ctx->rf_TM, sizeof(float) * l2 * chunk));
+    TRY(ensure(ctx, ctx->rf_F, sizeof(float2) * l2 * chunk));
+    TRY(ensure(ctx, ctx->rf_G, sizeof(float2) * l2 * chunk));
+    TRY(ensure(ctx, ctx->rf_TB, sizeof(float) * l2 * chunk));
+    TRY(ensure(ctx, ctx->rf_mask, sizeof(float) * l2));
+    k_ref_mask<<<blocks_for(l2, 256), 256, 0, ctx->stream>>>(P<float>(ctx->rf_mask), l, p.d_m);
+    ++ctx->counters.kernel_launches;
+    CKL();
+    RefineConsts rc;
+    rc.l = l;
+    rc.L2 = l2;
+    {
+        float ds = 0.0f;
+        CtfDev c0 = make_ctf(p, ctx->ctf0, p.window_size, &ds);
+        rc.apix = c0.apix; rc.lambda = c0.lambda; rc.cs = c0.cs; rc.ampconst = c0.ampconst;
+        rc.ds = ds;
+    }
+    rc.kk = p.kk; rc.a = p.a; rc.b = p.b; rc.b2 = p.b2;
+    rc.bf = p.bfactor; rc.bf2 = p.bfactor2; rc.bf3 = p.bfactor3;
+    rc.hp = ((float)l * p.apix) / p.highres;
+    rc.lp = ((float)l * p.apix) / p.lowres;
+    rc.d_m = p.d_m;
+    {
+        // bins with 0 <= shell < l/2 and x <= l/2 (the amplitude normalisation's count)
+        long long cnt = 0;
+        for (int y = 0; y < l; ++y)
+            for (int x = 0; x <= l / 2; ++x) {
+                const float dy = (float)std::min(y, l - y), dx = (float)std::min(x, l - x);
+                const int r = (int)floorf(hypotf(dy, dx) + 0.5f) - 1;
+                if (r >= 0 && r < l / 2) ++cnt;
+            }
+        rc.cnt = (float)cnt;
+    }
+    const float sgn = ((l / 2) % 2 == 0) ? 1.0f : -1.0f;
+    RefinePickDev* d_pk = P<RefinePickDev>(ctx->rf_pk);
+    RefineAcc* d_acc = P<RefineAcc>(ctx->rf_acc);
+    float2* B = P<float2>(ctx->rf_B);
+    float2* F1 = P<float2>(ctx->rf_F1);
+    float2* T = P<float2>(ctx->rf_T);
+    float* TM = P<float>(ctx->rf_TM);
+    float2* F = P<float2>(ctx->rf_F);
+    float2* Gm = P<float2>(ctx->rf_G);
+    float* TB = P<float>(ctx->rf_TB);
+    const float* mask = P<float>(ctx->rf_mask);
+    const float2* W = P<float2>(ctx->win);
+    const float inv_l2 = (float)(1.0 / (double)l2);
+    std::vector<RefinePickDev> hp(chunk);
+    std::vector<RefineAcc> ha(chunk);
+    for (int c0 = 0; c0 < n; c0 += chunk) {
+        const int nc = std::min(chunk, n - c0);
+        for (int i = 0; i < nc; ++i) {
+            const gs_refine_pick& q = picks[c0 + i];
+            RefinePickDev& d = hp[i];
+            d.window = q.window;
+            d.tmpl = q.template_index;
+            d.x0 = ((q.pos % l) - l / 2 + l) % l;
+            d.y0 = ((q.pos / l) - l / 2 + l) % l;
+            d.e = q.angle; d.dx = q.dx; d.dy = q.dy;
+            d.defocus = q.defocus; d.dfdiff = q.dfdiff; d.dfang = q.dfang;
+        }
+        CK(cudaMemcpyAsync(d_pk, hp.data(), sizeof(RefinePickDev) * nc, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemsetAsync(d_acc, 0, sizeof(RefineAcc) * nc, ctx->stream));
+        const dim3 g(blocks_for(l2, 256, 128), nc);
+        // forward
+        TRY(run_fft<false>(ctx, l, rows_of(l, l), nc, IoBaseIn{P<float>(ctx->tbase), d_pk, B, l2}));
+        TRY(run_fft<false>(ctx, l, cols_of(l, l), nc, IoComplex{B, inv_l2}));
+        k_ref_weight<<<g, 256, 0, ctx->stream>>>(B, F1, d_pk, rc, d_acc);
+        ++ctx->counters.kernel_launches;
+        TRY(run_fft<true>(ctx, l, rows_of(l, l), nc, IoInvA{F1, T, d_acc, rc.cnt, l2}));
+        TRY(run_fft<true>(ctx, l, cols_of(l, l), nc, IoComplex{T, 1.0f}));
+        k_ref_rotate<<<g, 256, 0, ctx->stream>>>(T, TM, d_pk, rc, mask, d_acc);
+        ++ctx->counters.kernel_launches;
+        TRY(run_fft<false>(ctx, l, rows_of(l, l), nc, IoNormIn{TM, d_acc, F, l2}));
+        TRY(run_fft<false>(ctx, l, cols_of(l, l), nc, IoComplex{F, inv_l2}));
+        k_ref_score<<<g, 256, 0, ctx->stream>>>(W, F, d_pk, rc, d_acc);
+        ++ctx->counters.kernel_launches;
+        CKL();
+        if (grad) {
+            TRY(run_fft<true>(ctx, l, rows_of(l, l), nc, IoFbarIn{W, F, d_pk, d_acc, Gm, l, l2, sgn}));
+            TRY(run_fft<true>(ctx, l, cols_of(l, l), nc, IoComplex{Gm, inv_l2}));
+            k_ref_gsum<<<g, 256, 0, ctx->stream>>>(Gm, TM, rc, d_acc);
+            ++ctx->counters.kernel_launches;
+            CK(cudaMemsetAsync(TB, 0, sizeof(float) * l2 * nc, ctx->stream));
+            k_ref_rot_adj<<<g, 256, 0, ctx->stream>>>(Gm, TM, T, d_pk, rc, mask, d_acc, TB);
+            ++ctx->counters.kernel_launches;
+            // Fbar2 = FFT(tbar), into Gm (gamma no longer needed)
+            TRY(run_fft<false>(ctx, l, rows_of(l, l), nc, IoRealIn2{TB, Gm}));
+            TRY(run_fft<false>(ctx, l, cols_of(l, l), nc, IoComplex{Gm, 1.0f}));
+            k_ref_abar<<<g, 256, 0, ctx->stream>>>(Gm, F1, rc, d_acc);
+            ++ctx->counters.kernel_launches;
+            k_ref_theta<<<g, 256, 0, ctx->stream>>>(Gm, F1, B, d_pk, rc, d_acc);
+            ++ctx->counters.kernel_launches;
+            CKL();
+            if (tgrad) {
+                // bbar = Re IFFT(Bbar) / l^2, real maps into TB
+                TRY(run_fft<true>(ctx, l, rows_of(l, l), nc, IoComplex{Gm, 1.0f}));
+                TRY(run_fft<true>(ctx, l, cols_of(l, l), nc, IoRealOut{Gm, TB, inv_l2}));
+                CK(cudaMemcpyAsync(tgrad + (size_t)c0 * l2, TB, sizeof(float) * l2 * nc, cudaMemcpyDeviceToHost,
+                                   ctx->stream));
+            }
+        }
+        CK(cudaMemcpyAsync(ha.data(), d_acc, sizeof(RefineAcc) * nc, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        for (int i = 0; i < nc; ++i) {
+            const RefineAcc& a = ha[i];
+            gs_refine_result& o = out[c0 + i];
+            const double sig = sqrt(a.sig2);
+            o.score = sig > 0.0 ? (float)(sgn * a.c / sig) : 0.0f;
+            o.d_angle = (float)a.de;
+            o.d_dx = sig > 0.0 ? (float)(sgn * a.cdx / sig) : 0.0f;
+            o.d_dy = sig > 0.0 ? (float)(sgn * a.cdy / sig) : 0.0f;
+            o.d_defocus = (float)a.dth[0];
+            o.d_dfdiff = (float)a.dth[1];
+            o.d_dfang = (float)a.dth[2];
+            if (!grad) o.d_angle = o.d_dx = o.d_dy = o.d_defocus = o.d_dfdiff = o.d_dfang = 0.0f;
+        }
+    }
+    return GS_OK;
+}
+
+// Gradient ascent of every pick's objective (no reference counterpart):
+// per step a move of length eta in scaled units (scale: 0.5 deg, 0.25 px,
+// 0.005 um, 0.005 um, 5 deg) along the scaled gradient; a step that lowers
+// the score is undone and eta halved for that pick.
+static int refine_impl(gs_ctx* ctx, gs_refine_pick* picks, int n, int steps, gs_refine_result* out) {
+    const double sc[6] = {0.5, 0.25, 0.25, 0.005, 0.005, 5.0};
+    std::vector<gs_refine_pick> cur(picks, picks + n), trial(cur);
+    std::vector<gs_refine_result> rc(n), rt(n);
+    std::vector<double> eta(n, 0.5);
+    TRY(score_grad_impl(ctx, cur.data(), n, true, rc.data(), nullptr));
+    auto get = [](const gs_refine_pick& q, int k) -> double {
+        switch (k) {
+            case 0: return q.angle;
+            case 1: return q.dx;
+            case 2: return q.dy;
+            case 3: return q.defocus;
+            case 4: return q.dfdiff;
+            default: return q.dfang;
+        }
+    };
+    auto set = [](gs_refine_pick& q, int k, double v) {
+        switch (k) {
+            case 0: q.angle = (float)v; break;
+            case 1: q.dx = (float)v; break;
+            case 2: q.dy = (float)v; break;
+            case 3: q.defocus = (float)v; break;
+            case 4: q.dfdiff = (float)v; break;
+            default: q.dfang = (float)v; break;
+        }
+    };
+    auto grad_of = [](const gs_refine_result& r, int k) -> double {
+        switch (k) {
+            case 0: return r.d_angle;
+            case 1: return r.d_dx;
+            case 2: return r.d_dy;
+            case 3: return r.d_defocus;
+            case 4: return r.d_dfdiff;
+            default: return r.d_dfang;
+        }
+    };
+    for (int it = 0; it < steps; ++it) {
+        for (int i = 0; i < n; ++i) {
+            double g2 = 0.0;
+            for (int k = 0; k < 6; ++k) {
+                const double gk = grad_of(rc[i], k) * sc[k];
+                g2 += gk * gk;
+            }
+            trial[i] = cur[i];
+            if (g2 > 0.0 && std::isfinite(g2)) {
+                const double norm = sqrt(g2);
+                for (int k = 0; k < 6; ++k)
+                    set(trial[i], k, get(cur[i], k) + eta[i] * sc[k] * sc[k] * grad_of(rc[i], k) / norm);
+            }
+            // keep the shift inside one pixel and the astigmatism magnitude non-negative
+            trial[i].dx = std::max(-1.0f, std::min(1.0f, trial[i].dx));
+            trial[i].dy = std::max(-1.0f, std::min(1.0f, trial[i].dy));
+            trial[i].dfdiff = std::max(0.0f, trial[i].dfdiff);
+        }
+        TRY(score_grad_impl(ctx, trial.data(), n, true, rt.data(), nullptr));
+        for (int i = 0; i < n; ++i) {
+            if (rt[i].score > rc[i].score) {
+                cur[i] = trial[i];
+                rc[i] = rt[i];
+            } else {
+                eta[i] *= 0.5;
+            }
+        }
+    }
+    for (int i = 0; i < n; ++i) {
+        picks[i] = cur[i];
+        out[i] = rc[i];
+    }
+    return GS_OK;
+}
+
 extern "C" {
 
 const char* gs_status_string(int s) {
@@ -575,7 +822,9 @@ int gs_ctx_destroy(gs_ctx* ctx) {
     DBuf* bufs[] = {&ctx->tmpl, &ctx->in, &ctx->q, &ctx->cimg, &ctx->img, &ctx->stats, &ctx->ra, &ctx->rb,
                     &ctx->off, &ctx->win, &ctx->wsum, &ctx->winv, &ctx->tspec, &ctx->scratch, &ctx->pstats,
                     &ctx->coef, &ctx->acc, &ctx->units, &ctx->picks, &ctx->count, &ctx->unit_wp,
-                    &ctx->dep_counters, &ctx->pacc, &ctx->flags};
+                    &ctx->dep_counters, &ctx->pacc, &ctx->flags, &ctx->tbase, &ctx->rf_pk, &ctx->rf_acc,
+                    &ctx->rf_B, &ctx->rf_F1, &ctx->rf_T, &ctx->rf_TM, &ctx->rf_F, &ctx->rf_G, &ctx->rf_TB,
+                    &ctx->rf_mask};
     for (DBuf* b : bufs) free_buf(*b);
     for (cudaEvent_t e : ctx->kev) cudaEventDestroy(e);
     cudaStreamDestroy(ctx->stream);
@@ -626,8 +875,9 @@ int gs_set_templates(gs_ctx* ctx, const gs_params* p, const float* host_template
     ctx->ty = ty;
     const size_t l2 = (size_t)l * l;
     TRY(ensure(ctx, ctx->tmpl, sizeof(float) * l2 * n));
+    TRY(ensure(ctx, ctx->tbase, sizeof(float) * l2 * n));
     const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)n, (size_t)(1u << 30) / (l2 * 8)));
-    DBuf raw, F, div, sumsq, inv, wmap;
+    DBuf raw, F, div, sumsq, inv, wmap, Fb;
     int st = GS_OK;
     do {
         if ((st = ensure(ctx, raw, sizeof(float) * (size_t)tx * ty * chunk))) break;
@@ -636,6 +886,7 @@ int gs_set_templates(gs_ctx* ctx, const gs_params* p, const float* host_template
         if ((st = ensure(ctx, sumsq, sizeof(double) * 2 * chunk))) break;
         if ((st = ensure(ctx, inv, sizeof(double) * chunk))) break;
         if ((st = ensure(ctx, wmap, sizeof(float) * l2))) break;
+        if ((st = ensure(ctx, Fb, sizeof(float2) * l2 * chunk))) break;
         // weight map with the FIRST micrograph's CTF; ds from the configured
         // window size (main.cu:155 runs before main.cu:1116 adjusts it)
         float ds = 0.0f;
@@ -669,6 +920,15 @@ int gs_set_templates(gs_ctx* ctx, const gs_params* p, const float* host_template
             cudaFuncSetAttribute(k_tmpl_shells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shs);
             k_tmpl_shells<<<nc, 256, shs, ctx->stream>>>(P<float2>(F), l, P<float>(div));
             ++ctx->counters.kernel_launches;
+            {
+                // whitened base (before the weight), kept for the refinement
+                dim3 gb(blocks_for((long long)l2, 256, 64), nc);
+                k_tmpl_whiten<<<gb, 256, 0, ctx->stream>>>(P<float2>(F), l, P<float>(div), P<float2>(Fb));
+                ++ctx->counters.kernel_launches;
+                if ((st = run_fft<true>(ctx, l, rows_of(l, l), nc, IoComplex{P<float2>(Fb), 1.0f}))) break;
+                if ((st = run_fft<true>(ctx, l, cols_of(l, l), nc,
+                                        IoRealOut{P<float2>(Fb), P<float>(ctx->tbase) + (size_t)c0i * l2, 1.0f}))) break;
+            }
             cudaMemsetAsync(P<double>(sumsq), 0, sizeof(double) * 2 * nc, ctx->stream);
             dim3 g(blocks_for((long long)l2, 256, 64), nc);
             k_tmpl_apply<<<g, 256, 0, ctx->stream>>>(P<float2>(F), l, P<float>(div), P<float>(wmap), P<double>(sumsq));
@@ -691,7 +951,7 @@ int gs_set_templates(gs_ctx* ctx, const gs_params* p, const float* host_template
         if (e != cudaSuccess) st = set_err(ctx, GS_ERR_CUDA, "template preprocessing: %s", cudaGetErrorString(e));
     } while (0);
     cudaStreamSynchronize(ctx->stream);
-    free_buf(raw); free_buf(F); free_buf(div); free_buf(sumsq); free_buf(inv); free_buf(wmap);
+    free_buf(raw); free_buf(F); free_buf(div); free_buf(sumsq); free_buf(inv); free_buf(wmap); free_buf(Fb);
     if (st == GS_OK) ctx->have_tmpl = true;
     return st;
 }
@@ -1378,6 +1638,24 @@ int gs_set_option(gs_ctx* ctx, int option, int value) {
         case GS_OPT_AUTOTUNE: ctx->autotune = value != 0; return GS_OK;
         default: return set_err(ctx, GS_ERR_ARG, "unknown option %d", option);
     }
+}
+
+int gs_score_grad(gs_ctx* ctx, const gs_refine_pick* picks, int n, int with_gradient, gs_refine_result* out,
+                  float* template_gradients) {
+    if (!ctx || (!picks && n > 0) || (!out && n > 0) || n < 0) return set_err(ctx, GS_ERR_ARG, "null pointer or n < 0");
+    if (n == 0) return GS_OK;
+    if (!ctx->have_tmpl) return set_err(ctx, GS_ERR_STATE, "gs_set_templates must come first");
+    CK(cudaSetDevice(ctx->device));
+    return score_grad_impl(ctx, picks, n, with_gradient != 0, out, with_gradient ? template_gradients : nullptr);
+}
+
+int gs_refine(gs_ctx* ctx, gs_refine_pick* picks, int n, int steps, gs_refine_result* out) {
+    if (!ctx || (!picks && n > 0) || (!out && n > 0) || n < 0 || steps < 0)
+        return set_err(ctx, GS_ERR_ARG, "null pointer, n < 0 or steps < 0");
+    if (n == 0) return GS_OK;
+    if (!ctx->have_tmpl) return set_err(ctx, GS_ERR_STATE, "gs_set_templates must come first");
+    CK(cudaSetDevice(ctx->device));
+    return refine_impl(ctx, picks, n, steps, out);
 }
 
 int gs_get_tuning(gs_ctx* ctx, int* out4) {

@@ -121,6 +121,25 @@ __global__ void k_weight_map(float* __restrict__ wmap, int l, WeightConsts wc, C
     wmap[i] = f;
 }
 
+// The whitened template spectrum alone (F / shell RMS, no weight), written
+// to B: the base that the off-grid refinement re-weights with other CTF
+// parameters.  Same whitening as k_tmpl_apply (whiten_Tmp, GPU_func.cu:130-152).
+__global__ void __launch_bounds__(256) k_tmpl_whiten(const float2* __restrict__ F, int l, const float* __restrict__ div,
+                                                     float2* __restrict__ B) {
+    const int J = blockIdx.y;
+    const int ns = l / 2;
+    const float2* d = F + (size_t)J * l * l;
+    const float* dv = div + (size_t)J * ns;
+    const int npix = l * l;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += gridDim.x * blockDim.x) {
+        const int x = i % l, y = i / l;
+        const int r = shell_index(x, y, l, l);
+        float2 v = d[i];
+        if (r >= 0 && r < ns) v = cscale(v, 1.0f / dv[r]);
+        B[(size_t)J * l * l + i] = v;
+    }
+}
+
 // Whiten by the shell RMS, apply the weight map, and accumulate per template
 // sum |F|^2 and the count over r < l/2, x <= l/2.
 // Reference: whiten_Tmp + apply_weighting_function + compute_area_sum_ofSQR

@@ -124,13 +124,21 @@ __device__ __forceinline__ bool tc_gemm(unsigned char* sm, uint32_t tmem, uint64
     return ok;
 }
 
-// Reads 8 complex outputs (kb = 8 q .. 8 q + 7) of this thread's GEMM row.
-__device__ __forceinline__ void tc_read8(uint32_t tmem, int q, float2* out) {
-    float f[16];
-    tc::tmem_ld16(tmem + ((uint32_t)(32 * (threadIdx.x >> 5)) << 16) + (uint32_t)(16 * q), f);
-    tc::tmem_ld_wait();
+// This thread's GEMM row (KP columns = KP / 2 complex outputs kb) from TMEM,
+// all loads issued before one wait.
+template <int KP>
+__device__ __forceinline__ void tc_read_row(uint32_t tmem, uint32_t* r) {
+    const uint32_t base = tmem + ((uint32_t)(32 * (threadIdx.x >> 5)) << 16);
 #pragma unroll
-    for (int i = 0; i < 8; ++i) out[i] = make_float2(f[2 * i], f[2 * i + 1]);
+    for (int q = 0; q < KP / 32; ++q) tc::tmem_ld32(base + 32 * q, r + 32 * q);
+    tc::tmem_ld_wait();
+}
+
+// Publishes one warp's share of a tile: its stores or atomics, then the
+// counter increment with release semantics.
+__device__ __forceinline__ void publish_warp(int* counter) {
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(counter) : "memory");
 }
 
 template <int N2, bool kBf16>
@@ -152,21 +160,12 @@ __device__ __forceinline__ bool tc_row_tile(const CorrArgs& a, int u, int t, uns
     const bool ok = tc_gemm<N2, kBf16>(sm, tmem, bar, phase);
     const int r = threadIdx.x, ka = r >> 3, v = r & 7;
     float2* dst = Rs + (long long)(r0 + v) * L + ka;
-#pragma unroll 1
-    for (int q = 0; q < (N2 + 7) / 8; ++q) {
-        float2 o[8];
-        tc_read8(tmem, q, o);
+    uint32_t o[C::KP];
+    tc_read_row<C::KP>(tmem, o);
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const int kb = 8 * q + i;
-            if (kb < N2) st_l2hint(dst + 16 * kb, o[i], keep);
-        }
-    }
-    __syncwarp();
-    if ((threadIdx.x & 31) == 0) {
-        __threadfence();
-        atomicAdd(&a.done_rows[u], 1);
-    }
+    for (int kb = 0; kb < N2; ++kb)
+        st_l2hint(dst + 16 * kb, make_float2(__uint_as_float(o[2 * kb]), __uint_as_float(o[2 * kb + 1])), keep);
+    publish_warp(&a.done_rows[u]);
     return ok;
 }
 
@@ -188,18 +187,15 @@ __device__ __forceinline__ bool tc_col_tile(const CorrArgs& a, int u, int t, uns
     float best1 = 0.0f, best2 = 0.0f;
     int bk1 = -1, bk2 = -1;
     float s1a = 0.f, s2a = 0.f, s1b = 0.f, s2b = 0.f;
-#pragma unroll 1
-    for (int q = 0; q < (N2 + 7) / 8; ++q) {
-        float2 o[8];
-        tc_read8(tmem, q, o);
+    {
+        uint32_t o[C::KP];
+        tc_read_row<C::KP>(tmem, o);
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const int kb = 8 * q + i;
-            if (kb >= N2) break;
+        for (int kb = 0; kb < N2; ++kb) {
             const int y = ka + 16 * kb;
             const bool in = xin && ((unsigned)(y - a.yb0) > (unsigned)(a.yb1 - a.yb0));
-            const float v1 = ((L / 2) % 2 == 0) ? o[i].x : -o[i].x;
-            const float v2 = ((L / 2) % 2 == 0) ? o[i].y : -o[i].y;
+            const float v1 = ((L / 2) % 2 == 0) ? __uint_as_float(o[2 * kb]) : -__uint_as_float(o[2 * kb]);
+            const float v2 = ((L / 2) % 2 == 0) ? __uint_as_float(o[2 * kb + 1]) : -__uint_as_float(o[2 * kb + 1]);
             const bool g1 = in && v1 > best1, g2 = in && v2 > best2;
             best1 = g1 ? v1 : best1;
             bk1 = g1 ? kb : bk1;
@@ -234,8 +230,9 @@ __device__ __forceinline__ bool tc_col_tile(const CorrArgs& a, int u, int t, uns
         if (kb_key) atomicMax(&ac[1].key, kb_key);
         atomicAdd(&ac[1].s1, d1b);
         atomicAdd(&ac[1].s2, d2b);
-        __threadfence();
-        last = atomicAdd(&a.done_cols[u], 1) == kTcWarps * C::T - 1;
+        int prev;
+        asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;" : "=r"(prev) : "l"(&a.done_cols[u]) : "memory");
+        last = prev == kTcWarps * C::T - 1;
     }
     *last_out = last;
     return ok;
@@ -297,7 +294,11 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(CorrArgs a) {
             *reinterpret_cast<uint32_t*>(smt + C::off_a_lo + off) = 0u;
         }
     }
-    if ((threadIdx.x >> 5) == 0) tc::tmem_alloc(tslot, C::tmem_cols);
+    if ((threadIdx.x >> 5) == 0) {
+        tc::tmem_alloc(tslot, C::tmem_cols);
+        // let the SM's other CTA allocate its columns while this one runs
+        tc::tmem_relinquish();
+    }
     if (threadIdx.x == 0) {
         tc::mbar_init(bar, 1);
         tc::fence_mbar_init();

@@ -194,6 +194,47 @@ void gs_picks_free(gs_pick* picks);
 #define GS_TIMING_COUNT 8
 int gs_get_timings(struct gs_ctx* ctx, float* out, int n);
 
+/* ---- Off-grid refinement (no reference counterpart) ----
+ * The objective of a pick continues the search's score off its grid: the
+ * template is re-weighted with the pick's CTF (defocus, dfdiff, dfang of the
+ * band-pass x |CTF| Wiener weight, main.cu:434-463), rotated by the pick's
+ * angle (the search's bilinear rotation, mask and normalisation,
+ * main.cu:669-716), and correlated with the window at the map position pos
+ * moved by (dx, dy) pixels (band-limited, through the window spectrum); the
+ * score is that correlation over the map's standard deviation (Parseval).
+ * At the grid angle, dx = dy = 0 and the CTF of the first micrograph it is the
+ * search's score up to the peak's own share of sigma (about 1e-4 relative).
+ * Picks refer to the window spectra of the last norm_type 0 search on this
+ * context (window: index in its window order, all micrographs of a batch in
+ * order; pos: the unit's peak position as gs_get_units reports it). */
+typedef struct gs_refine_pick {
+    int window;
+    int template_index;
+    int pos;               /* Y * l + X, map position of the peak */
+    float angle;           /* in-plane angle, degrees */
+    float dx, dy;          /* sub-pixel shift, pixels */
+    float defocus, dfdiff, dfang;  /* um (positive underfocus), um, degrees */
+} gs_refine_pick;
+
+typedef struct gs_refine_result {
+    float score;
+    float d_angle, d_dx, d_dy, d_defocus, d_dfdiff, d_dfang;  /* d score / d parameter */
+} gs_refine_result;
+
+/* Objective of n picks and, with with_gradient, its gradient by the adjoint
+ * (the forward's spectra are kept on the device for the backward of the same
+ * call; nothing is stored across calls).  template_gradients: null, or host
+ * memory of n x l x l floats receiving d score / d template base pixels (the
+ * whitened template before the CTF weight, l x l). */
+int gs_score_grad(struct gs_ctx* ctx, const gs_refine_pick* picks, int n, int with_gradient,
+                  gs_refine_result* out, float* template_gradients);
+
+/* `steps` steps of gradient ascent on every pick's objective (angle, shift,
+ * defocus, dfdiff, dfang); a step that lowers a pick's score is undone and
+ * that pick's step length halved.  picks are updated in place; out receives
+ * the final scores and gradients. */
+int gs_refine(struct gs_ctx* ctx, gs_refine_pick* picks, int n, int steps, gs_refine_result* out);
+
 /* Scheduling the last search used for the persistent correlation (after
  * autotuning when GS_OPT_AUTOTUNE is on): out4 = {ring slots, lag, window
  * block, CTAs per SM (0 = as many as fit)}. */

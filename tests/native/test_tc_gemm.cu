@@ -41,7 +41,10 @@ __global__ void __launch_bounds__(128) k_gemm(const float* __restrict__ A, const
         *reinterpret_cast<uint32_t*>(b_lo + tc::kmajor_off(r, k, N)) = lo;
     }
     tc::fence_async_smem();
-    if (warp == 0) tc::tmem_alloc(slot, 128);
+    if (warp == 0) {
+        tc::tmem_alloc(slot, 128);
+        tc::tmem_relinquish();
+    }
     if (tid == 0) {
         tc::mbar_init(bar, 1);
         tc::fence_mbar_init();
