@@ -273,11 +273,11 @@ int launch_corr_tc_n2(gs_ctx* ctx, const CorrArgs& a, long long total_items) {
     CK(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTcThreads, C::bytes));
     if (per_sm < 1) return set_err(ctx, GS_ERR_UNSUPPORTED, "tensor-core kernel does not fit on an SM");
-    // Two CTAs per SM fit (2 x 93 KB of shared memory, 2 x 128 TMEM columns)
-    // even where the occupancy query reports one.  Launching CTAs that cannot
+    // kCtasPerSm CTAs fit per SM (shared memory, registers and TMEM columns)
+    // even where the occupancy query reports fewer.  Launching CTAs that cannot
     // be resident is harmless here: a CTA claims work items only while it
     // runs, so no resident CTA ever waits on one that has not started.
-    per_sm = std::max(per_sm, 2);
+    per_sm = std::max(per_sm, C::kCtasPerSm);
     // TMEM: every resident CTA holds tmem_cols of the SM's 512 columns
     per_sm = std::min(per_sm, (int)(512 / C::tmem_cols));
     if (ctx->corr_ctas_override > 0) per_sm = std::min(per_sm, ctx->corr_ctas_override);

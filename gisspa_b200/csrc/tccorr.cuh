@@ -44,6 +44,12 @@ struct TcCfg {
     // about 2e4 at l <= 768.
     static constexpr float a_scale = kBf16 ? 1.0f : 0.0625f;
     static constexpr float b_scale = kBf16 ? 1.0f : 16.0f;
+    // products per K step: both operands split (hi*hi + lo*hi + hi*lo).  A
+    // DFT matrix rounded once to FP16 (hi*F + lo*F, one matrix copy less and
+    // three CTAs per SM) gives about 2e-4 score error and moves peaks between
+    // near-equal pixels, which changes picks; it is not used.
+    static constexpr int kProducts = 3;
+    static constexpr int kCtasPerSm = 2;
     // shared memory
     static constexpr size_t a_bytes = (size_t)M * KP * 2;   // one of hi / lo
     static constexpr size_t b_bytes = (size_t)KP * KP * 2;
@@ -51,7 +57,7 @@ struct TcCfg {
     static constexpr size_t off_a_lo = off_a_hi + a_bytes;
     static constexpr size_t off_b_hi = off_a_lo + a_bytes;
     static constexpr size_t off_b_lo = off_b_hi + b_bytes;
-    static constexpr size_t off_tw = off_b_lo + b_bytes;
+    static constexpr size_t off_tw = off_b_lo + (kProducts == 3 ? b_bytes : 0);
     static constexpr size_t off_bar = off_tw + (size_t)16 * N2 * sizeof(float2);
     static constexpr size_t off_misc = off_bar + 16;      // tmem slot + 4 broadcast slots
     static constexpr size_t bytes = off_misc + 32;
@@ -103,7 +109,8 @@ __device__ __forceinline__ void tc_issue(unsigned char* sm, uint32_t tmem, uint6
         tc::mma_f16(tmem, tc::smem_desc(a_hi + oa, lbo_a, 128), tc::smem_desc(b_hi + ob, lbo_b, 128), C::idesc, acc);
         acc = 1;
         tc::mma_f16(tmem, tc::smem_desc(a_lo + oa, lbo_a, 128), tc::smem_desc(b_hi + ob, lbo_b, 128), C::idesc, 1);
-        tc::mma_f16(tmem, tc::smem_desc(a_hi + oa, lbo_a, 128), tc::smem_desc(b_lo + ob, lbo_b, 128), C::idesc, 1);
+        if (C::kProducts == 3)
+            tc::mma_f16(tmem, tc::smem_desc(a_hi + oa, lbo_a, 128), tc::smem_desc(b_lo + ob, lbo_b, 128), C::idesc, 1);
     }
     tc::mma_commit(bar);
 }
@@ -251,7 +258,7 @@ __device__ __forceinline__ void tc_wait_for(const CorrArgs& a, int item) {
 }
 
 template <int N2, bool kBf16>
-__global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(CorrArgs a) {
+__global__ void __launch_bounds__(kTcThreads, TcCfg<N2, kBf16>::kCtasPerSm) k_corr_tc(CorrArgs a) {
     using C = TcCfg<N2, kBf16>;
     extern __shared__ __align__(128) unsigned char smt[];
     float2* twt = reinterpret_cast<float2*>(smt + C::off_tw);
@@ -283,7 +290,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(CorrArgs a) {
         tc::Split<kBf16>::run(e0, e1, hi, lo);
         const uint32_t off = tc::kmajor_off(row, col, C::KP);
         *reinterpret_cast<uint32_t*>(smt + C::off_b_hi + off) = hi;
-        *reinterpret_cast<uint32_t*>(smt + C::off_b_lo + off) = lo;
+        if (C::kProducts == 3) *reinterpret_cast<uint32_t*>(smt + C::off_b_lo + off) = lo;
     }
     // K padding of the A operand stays zero (step 1 writes only b < N2)
     for (int i = threadIdx.x; i < C::M * C::KP / 2; i += kTcThreads) {

@@ -92,6 +92,28 @@ def test_adjoint_matches_fp64_gradient(case):
     print("adjoint vs FP64 gradient: worst component error %.2e" % worst)
 
 
+def test_autograd_function_backward(case):
+    """The torch.autograd.Function wrapper: backward of sum(scores) gives the
+    adjoint's gradient, which matches the FP64 reference."""
+    torch = pytest.importorskip("torch")
+    from gisspa_b200.autograd import PickScore, PARAM_FIELDS
+    pk = _picks(case, 4, off_grid=True)
+    params = torch.tensor(np.stack([pk[f].astype(np.float64) for f in PARAM_FIELDS], axis=1),
+                          requires_grad=True)
+    s = PickScore.apply(params, case["ctx"], pk)
+    s.sum().backward()
+    for q in range(len(pk)):
+        p = pk[q]
+        _, ge, gd, gth, _ = R.score_and_grad(case["base"][p["template_index"]], case["W"][p["window"]],
+                                             RC.x0_of(int(p["pos"])), float(p["angle"]),
+                                             (float(p["dx"]), float(p["dy"])),
+                                             (float(p["defocus"]), float(p["dfdiff"]), float(p["dfang"])),
+                                             case["wc"], case["parts"], case["mask"])
+        ref = np.array([ge, gd[0], gd[1], gth[0], gth[1], gth[2]])
+        got = params.grad[q].numpy()
+        assert (np.abs(got - ref) <= 2e-3 * (np.abs(ref) + 1e-3 * np.linalg.norm(ref))).all(), (got, ref)
+
+
 def test_refinement_improves_grid_picks(case):
     pk = _picks(case, 24, off_grid=False)
     start = case["ctx"].score_grad(pk, with_gradient=False)["score"]
