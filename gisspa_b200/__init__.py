@@ -76,7 +76,7 @@ EXPORTS = ("gs_status_string", "gs_version", "gs_params_default", "gs_ctx_create
            "gs_search", "gs_search_device", "gs_get_units", "gs_picks_free", "gs_get_timings",
            "gs_get_stats", "gs_set_kernel_timing", "gs_set_option",
            "gs_correlate_window_noalloc", "gs_search_batch", "gs_get_tuning", "gs_score_grad",
-           "gs_refine")
+           "gs_refine", "gs_merge_duplicates")
 
 _lib_handle = None
 
@@ -128,6 +128,8 @@ def load_library(path: Optional[str] = None) -> C.CDLL:
     lib.gs_get_tuning.argtypes = [vp, C.POINTER(C.c_int)]
     lib.gs_score_grad.argtypes = [vp, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
     lib.gs_refine.argtypes = [vp, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+    lib.gs_merge_duplicates.argtypes = [C.c_int, C.c_void_p, C.c_size_t, C.c_double, C.c_double,
+                                        C.c_void_p]
     if path is None:
         _lib_handle = lib
     return lib
@@ -269,7 +271,7 @@ class Context:
         pk = np.array(picks, dtype=REFINE_PICK_DTYPE, copy=True)
         out = np.zeros(pk.shape[0], dtype=REFINE_RESULT_DTYPE)
         self._check(self._lib.gs_refine(self._h, pk.ctypes.data, pk.shape[0], int(steps), out.ctypes.data),
-                    "gs_refine")
+                    "gs_refine", "gs_merge_duplicates")
         return pk, out
 
     def _l(self) -> int:
@@ -353,6 +355,39 @@ class Context:
     def set_kernel_timing(self, enable: bool) -> None:
         self._check(self._lib.gs_set_kernel_timing(self._h, 1 if enable else 0),
                     "gs_set_kernel_timing")
+
+
+MERGE_ITEM_DTYPE = np.dtype([("x", "<f8"), ("y", "<f8"), ("alt", "<f8"), ("az", "<f8"),
+                             ("phi", "<f8"), ("score", "<f8"), ("group", "<i8")])
+MERGE_CLI_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "gisspa_merge")
+
+
+def merge_duplicates(items: np.ndarray, center: float, euler_thres: float, device: int = 0) -> np.ndarray:
+    """gs_merge_duplicates on MERGE_ITEM_DTYPE picks; returns the keep mask."""
+    it = np.ascontiguousarray(items, dtype=MERGE_ITEM_DTYPE)
+    keep = np.zeros(it.shape[0], dtype=np.uint8)
+    st = load_library().gs_merge_duplicates(int(device), it.ctypes.data, it.shape[0], float(center),
+                                            float(euler_thres), keep.ctypes.data)
+    if st != GS_OK:
+        raise GisspaError(st, "gs_merge_duplicates")
+    return keep.astype(bool)
+
+
+def merge_lines(lines, center: float, euler_thres: float, device: int = 0):
+    """Duplicate merging of pick lines (the reference's
+    remove_repeat_particles_from_list.py): the kept lines, in order."""
+    from . import formats
+    items = np.zeros(len(lines), dtype=MERGE_ITEM_DTYPE)
+    group, prev = -1, None
+    for k, line in enumerate(lines):
+        d = formats.parse_pick_line(line)
+        if d["path"] != prev:
+            group += 1
+            prev = d["path"]
+        items[k] = (d["center"][0], d["center"][1], d["euler"][0], d["euler"][1], d["euler"][2],
+                    d["score"], group)
+    keep = merge_duplicates(items, center, euler_thres, device)
+    return [l for l, k in zip(lines, keep) if k]
 
 
 NOALLOC_SCRATCH_BYTES = 32 << 20

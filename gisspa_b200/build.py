@@ -6,6 +6,7 @@
 Outputs
   gisspa_b200/lib/libgisspa_b200.so   C ABI of include/gisspa.h (CUDA kernels)
   gisspa_b200/lib/gisspa_main         drop-in CLI for the reference's ./main
+  gisspa_b200/lib/gisspa_merge        drop-in for its duplicate-merging script
 """
 from __future__ import annotations
 
@@ -22,6 +23,7 @@ LIBDIR = os.path.join(HERE, "lib")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(LIBDIR, "libgisspa_b200.so")
 DRIVER = os.path.join(LIBDIR, "gisspa_main")
+MERGE = os.path.join(LIBDIR, "gisspa_merge")
 
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -48,7 +50,8 @@ def build_library(force: bool = False) -> str:
     os.makedirs(LIBDIR, exist_ok=True)
     _run([NVCC] + NVCC_FLAGS + ARCH + ["-shared", "-I" + INCLUDE, "-o", LIB,
                                        os.path.join(CSRC, "gisspa.cu"),
-                                       os.path.join(CSRC, "noalloc.cu")])
+                                       os.path.join(CSRC, "noalloc.cu"),
+                                       os.path.join(CSRC, "merge.cu")])
     return LIB
 
 
@@ -60,6 +63,16 @@ def build_driver(force: bool = False) -> str:
     _run(["g++", "-O2", "-std=c++17", "-Wall", "-I" + INCLUDE] + dsrc +
          ["-L" + LIBDIR, "-lgisspa_b200", "-Wl,-rpath,$ORIGIN", "-o", DRIVER])
     return DRIVER
+
+
+def build_merge_cli(force: bool = False) -> str:
+    src = os.path.join(CSRC, "driver", "merge", "merge_main.cpp")
+    deps = [src, LIB, os.path.join(INCLUDE, "gisspa.h")]
+    if not force and _newer(MERGE, deps):
+        return MERGE
+    _run(["g++", "-O2", "-std=c++17", "-Wall", "-I" + INCLUDE, src,
+          "-L" + LIBDIR, "-lgisspa_b200", "-Wl,-rpath,$ORIGIN", "-o", MERGE])
+    return MERGE
 
 
 def build_reference_checker() -> bool:
@@ -75,6 +88,7 @@ def build_reference_checker() -> bool:
 def build_all(force: bool = False, reference: bool = True) -> None:
     build_library(force)
     build_driver(force)
+    build_merge_cli(force)
     if reference:
         build_reference_checker()
 

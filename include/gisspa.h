@@ -235,6 +235,26 @@ int gs_score_grad(struct gs_ctx* ctx, const gs_refine_pick* picks, int n, int wi
  * the final scores and gradients. */
 int gs_refine(struct gs_ctx* ctx, gs_refine_pick* picks, int n, int steps, gs_refine_result* out);
 
+/* ---- Duplicate merging of picks ----
+ * Replaces python_scripts/remove_repeat_particles_from_list.py: picks are
+ * grouped in runs of equal `group` (the script's runs of one micrograph
+ * path); inside a run, in order, two picks whose centres are closer than
+ * `center` pixels and whose orientations (alt, az, phi, degrees) are closer
+ * than `euler_thres` degrees (or than that modulo 180) are duplicates, and
+ * the lower score is removed (equal scores remove the earlier pick); a pick
+ * already removed when its turn comes is skipped.  keep[k] receives 1 for
+ * the picks that stay.  Pair tests run on `device` in FP64, the removal sweep
+ * on the host.  Needs no context. */
+typedef struct gs_merge_item {
+    double x, y;            /* centre, pixels */
+    double alt, az, phi;    /* orientation, degrees */
+    double score;
+    long long group;        /* run id (e.g. micrograph) */
+} gs_merge_item;
+
+int gs_merge_duplicates(int device, const gs_merge_item* items, size_t n, double center,
+                        double euler_thres, unsigned char* keep);
+
 /* Scheduling the last search used for the persistent correlation (after
  * autotuning when GS_OPT_AUTOTUNE is on): out4 = {ring slots, lag, window
  * block, CTAs per SM (0 = as many as fit)}. */
