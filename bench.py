@@ -59,6 +59,8 @@ def workload_kwargs(name: str, window: int = None):
         kw = synth.config_full(seed=1)
     elif name == "small":
         kw = synth.config_small(seed=0)
+    elif name == "batch":
+        kw = synth.config_batch(seed=2)
     else:
         raise ValueError(name)
     if window is not None:
@@ -332,6 +334,77 @@ def refinement_report(ctx, geom, m, n_picks=2048, steps=20, n_judge=256):
     return out
 
 
+def run_batch(args, rank, world, local_rank):
+    """The uneven batch (32 micrographs of three sizes, shared 1000 templates,
+    window 512) through gs_search_batch: one persistent launch per angle over
+    every window of every micrograph, the angle loop as one CUDA graph, the
+    scheduling autotuned on first use.  value = micrographs per second of the
+    whole batch; per-size rates from one-micrograph searches of each size."""
+    import numpy as np
+    import torch
+    import gisspa_b200 as G
+    from gisspa_b200 import build
+    if rank == 0:
+        build.build_library()
+    torch.cuda.set_device(local_rank)
+    ds, kw = make_data("batch", seed_offset=rank, templates=args.templates)
+    params = params_for(ds, kw)
+    if args.phistep:
+        params.phi_step = args.phistep
+    params.precision = PRECISION_MODES[args.precision]
+    mics = [m.image for m in ds.micrographs]
+    ctfs = [(m.defocus, m.dfdiff, m.dfang) for m in ds.micrographs]
+    ctx = G.Context(local_rank)
+    ctx.set_graph(True)
+    ctx.set_autotune(True)
+    ctx.set_templates(params, ds.templates, ctfs[0])
+    for _ in range(args.warmup):
+        ctx.search_batch(mics, ctfs)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    dev_ms = []
+    w0 = time.perf_counter()
+    for _ in range(args.steps):
+        picks = ctx.search_batch(mics, ctfs)
+        dev_ms.append(float(ctx.timings()[3]))
+    wall = (time.perf_counter() - w0) / args.steps
+    clocks = sampler.stop()
+    ms_step = float(np.mean(dev_ms))
+    ms_step, wall = reduce_max_over_ranks([ms_step, wall], world, f"cuda:{local_rank}")
+    if rank != 0:
+        ctx.close()
+        return None
+    per_size = {}
+    for size in sorted({m.shape for m in mics}):
+        k = next(i for i, m in enumerate(mics) if m.shape == size)
+        ctx.search(mics[k], ctfs[k])
+        t = float(ctx.timings()[3])
+        per_size["%dx%d" % (size[1], size[0])] = {"count": sum(m.shape == size for m in mics),
+                                                   "ms_alone": t, "micrographs_per_s_alone": 1000.0 / t}
+    g = ctx.geometry(mics[0].shape[1], mics[0].shape[0])
+    nm = len(mics)
+    line = {
+        "metric": METRIC, "value": world * nm * 1000.0 / ms_step, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": DTYPES[args.precision], "data": "synthetic",
+        "config": {"workload": "uneven batch: %d micrographs of 3838x3710 / 4096x4096 / 5760x4092, "
+                               "1000 templates 180x180, window 512 overlap 200, one search" % nm,
+                   "angles": g.n_angles, "templates": g.n_templates, "l": g.l,
+                   "reduced_for_profiling": bool(args.templates or args.phistep),
+                   "graph": True, "autotuned": list(ctx.tuning()),
+                   "parallelism": "replicas x%d" % world},
+        "e2e": {"value": world * nm / wall, "unit": UNIT,
+                "h2d_bytes_per_step": int(sum(m.size * 4 for m in mics)),
+                "d2h_bytes_per_step": int(32 * sum(len(p) for p in picks))},
+        "per_size": per_size,
+        "picks_per_batch": int(sum(len(p) for p in picks)),
+        "clocks": clocks,
+    }
+    ctx.close()
+    return line
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import gisspa_b200 as G
@@ -566,7 +639,7 @@ def main() -> int:
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["full", "small"], default="full")
+    ap.add_argument("--workload", choices=["full", "small", "batch"], default="full")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-refine", action="store_true", help="skip the off-grid refinement report")
     ap.add_argument("--no-tc-compare", action="store_true",
@@ -590,7 +663,10 @@ def main() -> int:
             torch.cuda.set_device(local_rank)
             dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                     device_id=torch.device("cuda", local_rank))
-        line = run_ours(args, rank, world, local_rank)
+        if args.workload == "batch":
+            line = run_batch(args, rank, world, local_rank)
+        else:
+            line = run_ours(args, rank, world, local_rank)
         if world > 1:
             import torch.distributed as dist
             dist.barrier()

@@ -280,6 +280,23 @@ def config_small(seed: int = 0) -> Dict[str, object]:
                 window=512, overlap=128, defocus=(1.5, 1.5), threshold=7.0)
 
 
+BATCH_SIZES = ((3838, 3710), (4096, 4096), (5760, 4092))
+
+
+def config_batch(seed: int = 2, n_micrographs: int = 32) -> Dict[str, object]:
+    """Uneven batch: n micrographs with sizes drawn (seeded) from 3838 x 3710,
+    4096 x 4096 and 5760 x 4092, 250 particles each at SNR 0.03, per-micrograph
+    defocus 0.8-2.5 um with up to 500 A astigmatism, 1/f^0.5 noise; one shared
+    set of 1000 templates 180^2 from an 800-blob density in a 90-px ball;
+    72 angles; window 512, overlap 200."""
+    rng = np.random.default_rng(seed + 1000)
+    sizes = [BATCH_SIZES[int(k)] for k in rng.integers(0, len(BATCH_SIZES), n_micrographs)]
+    return dict(seed=seed, nx=sizes[0][0], ny=sizes[0][1], sizes=sizes, n_micrographs=n_micrographs,
+                n_templates=1000, tsize=180, n_particles=250, snr=0.03, n_blobs=800, ball_radius=90.0,
+                phistep=5.0, diameter=170.0, window=512, overlap=200, defocus=(0.8, 2.5),
+                astig_A=500.0, noise_alpha=0.5, threshold=7.0, fast=True)
+
+
 def config_full(seed: int = 1, window: int = 720) -> Dict[str, object]:
     """5760 x 4092 micrograph, 400 particles at SNR 0.03, 2000 templates 200^2
     from an 800-blob density in a 90-px ball, 72 angles, defocus 0.8-2.5 um
