@@ -424,6 +424,8 @@ def run_ours(args, rank, world, local_rank):
         params.phi_step = args.phistep
     params.precision = PRECISION_MODES[args.precision]
     ctx = G.Context(local_rank)
+    if args.autotune:
+        ctx.set_autotune(True)   # tuned during the first warm-up search
     t0 = time.perf_counter()
     ctx.set_templates(params, ds.templates, ctf)
     t_tmpl = time.perf_counter() - t0
@@ -529,6 +531,8 @@ def run_ours(args, rank, world, local_rank):
                    "units_per_micrograph": na * nw * nt,
                    "reduced_for_profiling": bool(args.templates or args.phistep),
                    "parallelism": "replicas x%d" % world,
+                   "scheduling": {"autotuned": bool(args.autotune), "ring_slots_lag_window_block_ctas":
+                                  list(ctx.tuning())},
                    "l2": "inputs larger than L2 (template set %.1f GB, pair spectra %.1f GB per angle)"
                          % (nt * l2 * 4 / 1e9, npairs * l2 * 8 / 1e9)},
         "e2e": {"value": world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": nx * ny * 4,
@@ -642,6 +646,8 @@ def main() -> int:
     ap.add_argument("--workload", choices=["full", "small", "batch"], default="full")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-refine", action="store_true", help="skip the off-grid refinement report")
+    ap.add_argument("--autotune", action="store_true",
+                    help="let the scheduling autotuner pick ring slots, lag, window block, CTAs per SM")
     ap.add_argument("--no-tc-compare", action="store_true",
                     help="skip the FP32 vs tensor-core comparison over three angles")
     ap.add_argument("--precision", choices=sorted(PRECISION_MODES), default="fp32",
