@@ -125,10 +125,14 @@ __device__ __forceinline__ bool tc_gemm(unsigned char* sm, uint32_t tmem, uint64
     tc::fence_after_sync();
     tc_issue<N2, kBf16>(sm, tmem, bar);
     __syncwarp();
-    const bool ok = tc::mbar_wait(bar, phase, 1u << 24);
+    // one lane per warp polls the barrier (128 pollers of one shared word
+    // throttle the shared-memory pipe); the warp then synchronises with it
+    int ok = 1;
+    if ((threadIdx.x & 31) == 0) ok = tc::mbar_wait(bar, phase, 1u << 24) ? 1 : 0;
+    ok = __shfl_sync(0xffffffffu, ok, 0);
     phase ^= 1u;
     tc::fence_after_sync();
-    return ok;
+    return ok != 0;
 }
 
 // This thread's GEMM row (KP columns = KP / 2 complex outputs kb) from TMEM,

@@ -1,0 +1,81 @@
+"""The adjoint on the full-size workload: the 64 best units of a search of the
+5760 x 4092 micrograph (2000 templates 200^2, window 720), moved off the grid
+(angle + 0.37 deg, shift (0.13, -0.21) px, defocus + 137 A, astigmatism
++ 30 A at + 7 deg), against the FP64 reference gradient
+(oracle/refine_fp64.py) and central finite differences of it.  Several
+minutes of CPU (FP64 objective at l = 720): set GISSPA_SLOW=1."""
+import os
+
+import numpy as np
+import pytest
+
+import gisspa_b200 as G
+from gisspa_b200 import synth
+from oracle import gisspa_oracle as O
+from oracle import refine_fp64 as R
+
+pytestmark = [pytest.mark.gpu, pytest.mark.slow,
+              pytest.mark.skipif(os.environ.get("GISSPA_SLOW") != "1", reason="set GISSPA_SLOW=1")]
+
+
+def test_adjoint_full_size_64_picks():
+    kw = synth.config_full(seed=1)
+    seed = kw.pop("seed")
+    ds = synth.make_dataset(seed, **kw)
+    m = ds.micrographs[0]
+    ctf = (m.defocus, m.dfdiff, m.dfang)
+    p = ds.params
+    gp = G.default_params(apix=float(p["angpix"]), phi_step=float(p["phistep"]), kk=float(p["kk"]),
+                          energy=float(p["energy"]), cs=float(p["cs"]), highres=float(p["Highres"]),
+                          lowres=float(p["Lowres"]), d_m=float(p["diameter"]), thres=float(p["threshold"]),
+                          window_size=int(p["window_size"]), overlap=int(p["overlap"]),
+                          phase_flip=int(p["phase_flip"]))
+    l = 720
+    with G.Context(0) as ctx:
+        ctx.set_templates(gp, ds.templates, ctf)
+        ctx.search(m.image, ctf)
+        g = ctx.geometry(m.image.shape[1], m.image.shape[0])
+        na, nw, nt = g.n_angles, g.n_windows_x * g.n_windows_y, g.n_templates
+        u = ctx.units((na, nw, nt))
+        sc = np.where(np.isfinite(u["score"]), u["score"], -np.inf)
+        top = [np.unravel_index(i, sc.shape) for i in np.argsort(sc, axis=None)[::-1][:64]]
+        pk = np.zeros(len(top), dtype=G.REFINE_PICK_DTYPE)
+        for q, (ai, w, J) in enumerate(top):
+            pk[q] = (w, J, int(u["pos"][ai, w, J]), ai * 360.0 / na + 0.37, 0.13, -0.21,
+                     m.defocus + 0.0137, m.dfdiff + 0.003, m.dfang + 7.0)
+        res = ctx.score_grad(pk, with_gradient=True)
+    op = O.Params(apix=float(p["angpix"]), phi_step=float(p["phistep"]), kk=float(p["kk"]),
+                  energy=float(p["energy"]), cs=float(p["cs"]), highres=float(p["Highres"]),
+                  lowres=float(p["Lowres"]), d_m=float(p["diameter"]), thres=0.0, padding_size=l,
+                  phase_flip=1, overlap=int(p["overlap"]))
+    octf = O.make_ctf(op, *ctf, l)
+    img = O.preprocess_micrograph(m.image, op, octf, workers=8)
+    offx = O.window_offsets(m.image.shape[1], l, op.overlap)
+    offy = O.window_offsets(m.image.shape[0], l, op.overlap)
+    wins = sorted({int(x) for x in pk["window"]})
+    W = {}
+    for w in wins:
+        sub = O.split_windows(img, [offx[w % len(offx)]], [offy[w // len(offx)]], l)
+        W[w] = O.window_spectra(sub, op, workers=8)[0]
+    tids = sorted({int(x) for x in pk["template_index"]})
+    base = dict(zip(tids, R.template_base(ds.templates[tids], l)))
+    wc = R.weight_consts(op, l, octf)
+    parts = R.weight_parts(wc)
+    mask = O.soft_mask(l, op.d_m)
+    worst, worst_s = 0.0, 0.0
+    for q in range(len(pk)):
+        pq = pk[q]
+        x0 = (((int(pq["pos"]) % l) - l // 2) % l, ((int(pq["pos"]) // l) - l // 2) % l)
+        s, ge, gd, gth, _ = R.score_and_grad(base[int(pq["template_index"])], W[int(pq["window"])], x0,
+                                             float(pq["angle"]), (float(pq["dx"]), float(pq["dy"])),
+                                             (float(pq["defocus"]), float(pq["dfdiff"]), float(pq["dfang"])),
+                                             wc, parts, mask)
+        ref = np.array([ge, gd[0], gd[1], gth[0], gth[1], gth[2]])
+        got = np.array([res[f][q] for f in ("d_angle", "d_dx", "d_dy", "d_defocus", "d_dfdiff", "d_dfang")])
+        err = np.abs(got - ref) / (np.abs(ref) + 1e-3 * np.linalg.norm(ref))
+        worst = max(worst, float(err.max()))
+        worst_s = max(worst_s, abs(float(res["score"][q]) - s) / abs(s))
+    print("full-size adjoint, 64 picks: worst score error %.2e, worst gradient component error %.2e"
+          % (worst_s, worst))
+    assert worst_s <= 1e-4
+    assert worst <= 2e-3
