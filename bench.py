@@ -234,6 +234,9 @@ DTYPES = {"fp32": "f32", "tc-bf16": "bf16 hi+lo split, f32 accumulate",
           "tc-fp16": "fp16 hi+lo split, f32 accumulate"}
 
 
+TRAFFIC_PER_PAIR_UNIT_L720 = (10500180992 + 60203776) / 8800.0
+
+
 def tensor_core_comparison(ds, kw, local_rank, base_precision: str):
     """The two correlation paths on the same micrograph and templates over
     three in-plane angles (0, 120, 240 deg): per-angle correlation time of
@@ -496,9 +499,16 @@ def run_ours(args, rank, world, local_rank):
         hbm_bytes = (npairs * math.ceil(nw / wblk) + nw) * l2 * 8.0   # P once per window block, W once
         kname = ("k_corr_persistent (row + column tiles of one angle)" if args.precision == "fp32" else
                  "k_corr_tc (row + column tiles of one angle; N2-point DFT stage on the tensor cores)")
+        # DRAM traffic of the persistent FP32 kernel per (window, pair) unit at
+        # l = 720, from one ncu capture of a 100-pair launch
+        # (profiles/k_corr_persistent_l720_100pairs.md: 10.50 GB read + 0.06 GB
+        # written for 8800 units), scaled to this launch's units
+        traffic = (TRAFFIC_PER_PAIR_UNIT_L720 * npairs * nw
+                   if (l == 720 and args.precision == "fp32") else None)
         roof = {"bound": "fp32", "kernel": kname,
                 "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                "traffic": None, "peak_source": "148 SMs x 256 FLOP/clk x median SM clock under load",
+                "traffic": traffic, "traffic_source": "ncu capture of 100 pairs, scaled by units" if traffic else None,
+                "peak_source": "148 SMs x 256 FLOP/clk x median SM clock under load",
                 "algorithmic_flops_per_launch": flops_launch, "avg_launch_ms": avg_ms, "launches": kn,
                 "kernel_share_of_step": kms / (ms_step * args.steps),
                 "hbm": {"algorithmic_bytes_per_launch": hbm_bytes,

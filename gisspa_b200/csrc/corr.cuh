@@ -110,6 +110,13 @@ __device__ __forceinline__ void st_l2hint(float2* ptr, float2 v, unsigned long l
                  :: "l"(ptr), "f"(v.x), "f"(v.y), "l"(pol) : "memory");
 }
 
+// Drops one 128-byte line from L2 without writing it back (its contents
+// become undefined).  Used on scratch-map lines that have been consumed and
+// will be rewritten before they are read again.
+__device__ __forceinline__ void l2_discard128(const void* p) {
+    asm volatile("discard.global.L2 [%0], 128;" ::"l"(p) : "memory");
+}
+
 template <int N2>
 __device__ __forceinline__ void corr_row_tile(const CorrArgs& a, int u, int t, float2* tile, const float2* twt) {
     using F = Fast16<N2>;
@@ -183,6 +190,10 @@ __device__ __forceinline__ void corr_col_tile(const CorrArgs& a, int u, int t, f
         });
     }
     __syncthreads();
+    // every line of this tile's 16 columns has been read (the barrier orders
+    // the loads before the discards): drop them from L2 instead of letting
+    // them be written back; the slot is rewritten before its next read
+    for (int r = threadIdx.x; r < L; r += F::kThreads) l2_discard128(Rs + (long long)r * L + c0);
     const int v = threadIdx.x & 15, k1 = threadIdx.x >> 4;
     const int x = c0 + v;
     const bool xin = (unsigned)(x - a.yb0) > (unsigned)(a.yb1 - a.yb0);  // column outside the border
