@@ -158,7 +158,7 @@ class ClockSampler:
 def reduce_max_over_ranks(values, world: int, device=None):
     """Element-wise max of per-rank values over all ranks (no-op for one rank).
     The timed region's device time is the max over ranks, so replicas are
-    judged by the slowest GPU."""
+    timed by the slowest GPU."""
     if world <= 1:
         return [float(v) for v in values]
     import torch
@@ -282,10 +282,10 @@ def tensor_core_comparison(ds, kw, local_rank, base_precision: str):
     return out
 
 
-def refinement_report(ctx, geom, m, n_picks=2048, steps=20, n_judge=256):
+def refinement_report(ctx, geom, m, n_picks=2048, steps=20, n_grid=256):
     """Off-grid refinement of the search's best units (gs_refine) on the
     headline micrograph: time, share of picks whose score rises over the grid
-    score, and a judge: for n_judge picks the best score of a dense local grid
+    score, and a check against a dense local grid: for n_grid picks its best score
     (angle +-1 deg in 0.5 deg, shift +-0.5 px in 0.25 px, defocus +-100 A in
     50 A; 625 points, evaluated through gs_score_grad) against the refined
     score."""
@@ -310,7 +310,7 @@ def refinement_report(ctx, geom, m, n_picks=2048, steps=20, n_judge=256):
            "improved_frac": float((gain > 1e-6 * np.abs(start)).mean()),
            "lowered": int((gain < -1e-6 * np.abs(start)).sum()),
            "median_gain": float(np.median(gain)), "median_grid_score": float(np.median(start))}
-    nj = min(n_judge, len(pk))
+    nj = min(n_grid, len(pk))
     offs_a = np.arange(-2, 3) * 0.5
     offs_d = np.arange(-2, 3) * 0.25
     offs_f = np.arange(-2, 3) * 0.005
@@ -330,7 +330,7 @@ def refinement_report(ctx, geom, m, n_picks=2048, steps=20, n_judge=256):
     gs = ctx.score_grad(grid, with_gradient=False)["score"].reshape(nj, -1)
     t4 = time.perf_counter()
     best = gs.max(axis=1)
-    out["judge"] = {"picks": nj, "grid": "5 angles (0.5 deg) x 5 x 5 shifts (0.25 px) x 5 defocus (50 A)",
+    out["local_grid"] = {"picks": nj, "grid": "5 angles (0.5 deg) x 5 x 5 shifts (0.25 px) x 5 defocus (50 A)",
                     "grid_s": t4 - t3,
                     "refined_ge_grid_best_frac": float((res["score"][:nj] >= best - 1e-4 * np.abs(best)).mean()),
                     "median_refined_minus_grid_best": float(np.median(res["score"][:nj] - best))}
@@ -588,10 +588,8 @@ def run_reference(args, rank, world):
     from gisspa_b200 import synth
     binary = os.path.join(ROOT, "oracle", "_ref", "gisspa_ref")
     if not os.path.exists(binary):
-        if os.path.isdir("/root/reference"):
-            subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
-        if not os.path.exists(binary):
-            return {"impl": "reference", "unavailable": "reference build oracle/_ref/gisspa_ref not present"}
+        # built from the reference's sources by gisspa_b200.build (oracle/Makefile)
+        return {"impl": "reference", "unavailable": "reference build oracle/_ref/gisspa_ref not present"}
     window = 768 if args.workload == "full" else 512
     ds, kw = make_data(args.workload, window=window)
     work = tempfile.mkdtemp(prefix="gisspa_refbench_")

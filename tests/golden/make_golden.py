@@ -113,7 +113,7 @@ def run_reference(binary: str, name: str, workdir: str) -> dict:
 
 def main() -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
+    ap.add_argument("--out", default=None, help="directory for the <case>.json.gz files")
     ap.add_argument("--binary", default=os.path.join(ROOT, "oracle", "_ref", "gisspa_ref"))
     ap.add_argument("--cases", nargs="*", default=list(CASES))
     ap.add_argument("--list", action="store_true")
@@ -121,6 +121,8 @@ def main() -> int:
     if a.list:
         print("\n".join(CASES))
         return 0
+    if not a.out:
+        ap.error("--out is required")
     os.makedirs(a.out, exist_ok=True)
     work = tempfile.mkdtemp(prefix="gisspa_golden_")
     rc = 0
