@@ -271,18 +271,12 @@ int launch_corr_tc_n2(gs_ctx* ctx, const CorrArgs& a, long long total_items) {
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     CK(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTcThreads, C::bytes));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, C::kThreads, C::bytes));
     if (per_sm < 1) return set_err(ctx, GS_ERR_UNSUPPORTED, "tensor-core kernel does not fit on an SM");
-    // kCtasPerSm CTAs fit per SM (shared memory, registers and TMEM columns)
-    // even where the occupancy query reports fewer.  Launching CTAs that cannot
-    // be resident is harmless here: a CTA claims work items only while it
-    // runs, so no resident CTA ever waits on one that has not started.
-    per_sm = std::max(per_sm, C::kCtasPerSm);
-    // TMEM: every resident CTA holds tmem_cols of the SM's 512 columns
-    per_sm = std::min(per_sm, (int)(512 / C::tmem_cols));
-    if (ctx->corr_ctas_override > 0) per_sm = std::min(per_sm, ctx->corr_ctas_override);
-    const long long grid = std::min<long long>((long long)nsm * per_sm, total_items);
-    kern<<<(unsigned)grid, kTcThreads, C::bytes, ctx->stream>>>(a);
+    // one CTA per SM: it runs C::kWg pipelines and holds the TMEM columns of
+    // all of them (a second CTA would not fit in shared memory)
+    const long long grid = std::min<long long>((long long)nsm, total_items);
+    kern<<<(unsigned)grid, C::kThreads, C::bytes, ctx->stream>>>(a);
     ++ctx->counters.kernel_launches;
     CKL();
     return GS_OK;
