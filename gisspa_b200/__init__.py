@@ -271,7 +271,7 @@ class Context:
         pk = np.array(picks, dtype=REFINE_PICK_DTYPE, copy=True)
         out = np.zeros(pk.shape[0], dtype=REFINE_RESULT_DTYPE)
         self._check(self._lib.gs_refine(self._h, pk.ctypes.data, pk.shape[0], int(steps), out.ctypes.data),
-                    "gs_refine", "gs_merge_duplicates")
+                    "gs_refine")
         return pk, out
 
     def _l(self) -> int:
