@@ -125,7 +125,7 @@ def load_library(path: Optional[str] = None) -> C.CDLL:
                                     C.POINTER(C.c_int), C.POINTER(GsCtf),
                                     C.POINTER(C.POINTER(GsPick)), C.POINTER(C.c_size_t),
                                     C.POINTER(C.c_size_t)]
-    lib.gs_get_tuning.argtypes = [vp, C.POINTER(C.c_int)]
+    lib.gs_get_tuning.argtypes = [vp, C.POINTER(C.c_int), C.c_int]
     lib.gs_score_grad.argtypes = [vp, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
     lib.gs_refine.argtypes = [vp, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
     lib.gs_merge_duplicates.argtypes = [C.c_int, C.c_void_p, C.c_size_t, C.c_double, C.c_double,
@@ -290,11 +290,15 @@ class Context:
         """Resident CTAs per SM of the persistent kernel (0 = as many as fit)."""
         self._check(self._lib.gs_set_option(self._h, 6, int(per_sm)), "gs_set_option")
 
-    def tuning(self) -> Tuple[int, int, int, int]:
-        """(ring slots, lag, window block, CTAs per SM) of the last search."""
-        t = (C.c_int * 4)()
-        self._check(self._lib.gs_get_tuning(self._h, t), "gs_get_tuning")
+    def tuning(self) -> Tuple[int, int, int, int, int]:
+        """(ring slots, lag, window block, CTAs per SM, tile width) of the last search."""
+        t = (C.c_int * 5)()
+        self._check(self._lib.gs_get_tuning(self._h, t, 5), "gs_get_tuning")
         return tuple(t[:])
+
+    def set_corr_tile(self, vectors: int) -> None:
+        """Tile width of the FP32 persistent kernel (16 or 8 vectors)."""
+        self._check(self._lib.gs_set_option(self._h, 9, int(vectors)), "gs_set_option")
 
     def search_device(self, dev_ptr: int, nx: int, ny: int, ctf) -> np.ndarray:
         ptr = C.POINTER(GsPick)()

@@ -2,20 +2,22 @@
 // (window, template pair) unit of one in-plane angle in a single launch.
 //
 // Work items, claimed in increasing order from one atomic counter:
-//   slot s (0 <= s < Nu + lag) = [N2 row tiles of unit s] [N2 column tiles of unit s - lag]
-// A row tile takes 16 spectrum rows of unit u: S = W_w conj(P_p), inverse FFT
-// along x (fastfft.cuh four-step), written to scratch map slot u % S.  A
-// column tile takes 16 columns of that map: inverse FFT along y and the score
+//   slot s (0 <= s < Nu + lag) = [T row tiles of unit s] [T column tiles of unit s - lag]
+// with T = l / V tiles of V vectors (V = 16 or 8, CorrCfg).  A row tile takes V
+// spectrum rows of unit u: S = W_w conj(P_p), inverse FFT along x (the
+// four-step l = 16 N2 transform of fastfft.cuh), written to scratch map slot
+// u % S.  A column tile takes V columns of that map: inverse FFT along y and the score
 // epilogue (border-masked peak and position, sum and sum of squares of both
 // templates of the pair), reduced into the unit's accumulators; the last
 // column tile of a unit computes the two scores.
 //
 // Dependencies and why they cannot deadlock: a column tile of u waits until
-// all N2 row tiles of u are done; a row tile of u >= S waits until all
+// all T row tiles of u are done; a row tile of u >= S waits until all
 // column tiles of u - S are done (its scratch slot is free).  Completion is
 // counted per warp (every warp of a tile fences its own stores or atomics and
-// increments the unit's counter), so a unit is done at 8 N2 increments and no
-// CTA-wide barrier is needed to publish a tile.  Both wait only
+// increments the unit's counter), so a pass of a unit is done at
+// (warps per CTA) x T increments and no CTA-wide barrier is needed to
+// publish a tile.  Both wait only
 // on items that come earlier in the claim order, and an item is claimed only
 // by a running CTA that finishes it before claiming another, so the earliest
 // unfinished item can always proceed.  Every wait is bounded; a wait that
@@ -74,12 +76,28 @@ __device__ __forceinline__ void wait_counter(const int* p, int target, int* erro
     atomicExch(error, 1);
 }
 
-constexpr int kCorrWarps = 8;  // warps per CTA (256 threads)
+// Tile geometry: V vectors per tile (16 or 8), 16 V threads per CTA (step 2
+// has one (vector, k1) task per thread), 512 / (16 V) CTAs per SM.  A pass of
+// one unit is T = L / V tiles and kDone = (warps per CTA) x T per-warp
+// completions, the same count (8 N2 x 45 / N2 ...) for both widths.
+template <int N2, int V_>
+struct CorrCfg {
+    static constexpr int L = 16 * N2;
+    static constexpr int V = V_;
+    static constexpr int BP = (N2 % 2) ? N2 : N2 + 1;  // odd block pitch
+    static constexpr int VP = 16 * BP + 1;             // vector pitch
+    static constexpr int kThreads = 16 * V;
+    static constexpr int kWarps = kThreads / 32;
+    static constexpr int T = L / V;
+    static constexpr int kDone = kWarps * T;
+    static constexpr int kCtasPerSm = 512 / kThreads;
+    static_assert(V == 8 || V == 16, "tile width");
+};
 
-template <int N2>
+template <int N2, int V>
 struct CorrSmem {
-    using F = Fast16<N2>;
-    static constexpr size_t tile = (size_t)F::V * F::VP * sizeof(float2);
+    using C = CorrCfg<N2, V>;
+    static constexpr size_t tile = (size_t)C::V * C::VP * sizeof(float2);
     static constexpr size_t tw = (size_t)16 * N2 * sizeof(float2);
     static constexpr size_t red = 128 * sizeof(double);
     static constexpr size_t bytes = tile + tw + red + 32;
@@ -117,9 +135,9 @@ __device__ __forceinline__ void l2_discard128(const void* p) {
     asm volatile("discard.global.L2 [%0], 128;" ::"l"(p) : "memory");
 }
 
-template <int N2>
+template <int N2, int V>
 __device__ __forceinline__ void corr_row_tile(const CorrArgs& a, int u, int t, float2* tile, const float2* twt) {
-    using F = Fast16<N2>;
+    using F = CorrCfg<N2, V>;
     constexpr int L = F::L;
     const int2 wp = a.unit_wp[u];
     const float2* Wr = a.W + (long long)wp.x * a.L2;
@@ -165,10 +183,10 @@ __device__ __forceinline__ void corr_row_tile(const CorrArgs& a, int u, int t, f
     }
 }
 
-template <int N2>
+template <int N2, int V>
 __device__ __forceinline__ void corr_col_tile(const CorrArgs& a, int u, int t, float2* tile, const float2* twt,
                                               bool* last_out) {
-    using F = Fast16<N2>;
+    using F = CorrCfg<N2, V>;
     constexpr int L = F::L;
     constexpr int h = L / 2;
     const float2* Rs = a.R + (long long)(u % a.S) * a.L2;
@@ -192,9 +210,14 @@ __device__ __forceinline__ void corr_col_tile(const CorrArgs& a, int u, int t, f
     __syncthreads();
     // every line of this tile's 16 columns has been read (the barrier orders
     // the loads before the discards): drop them from L2 instead of letting
-    // them be written back; the slot is rewritten before its next read
-    for (int r = threadIdx.x; r < L; r += F::kThreads) l2_discard128(Rs + (long long)r * L + c0);
-    const int v = threadIdx.x & 15, k1 = threadIdx.x >> 4;
+    // them be written back; the slot is rewritten before its next read.  An
+    // 8-column tile owns only half of each line and leaves them alone.
+    if (V == 16)
+        for (int r = threadIdx.x; r < L; r += F::kThreads) l2_discard128(Rs + (long long)r * L + c0);
+    // step-2 task: (vector, k1); both orders read distinct banks per half-warp
+    // for their width
+    const int v = V == 16 ? (threadIdx.x & 15) : (threadIdx.x >> 4);
+    const int k1 = V == 16 ? (threadIdx.x >> 4) : (threadIdx.x & 15);
     const int x = c0 + v;
     const bool xin = (unsigned)(x - a.yb0) > (unsigned)(a.yb1 - a.yb0);  // column outside the border
     float best1 = 0.0f, best2 = 0.0f;   // reference peak = max(0, masked max)
@@ -250,7 +273,7 @@ __device__ __forceinline__ void corr_col_tile(const CorrArgs& a, int u, int t, f
         atomicAdd(&ac[1].s1, d1b);
         atomicAdd(&ac[1].s2, d2b);
         __threadfence();
-        last = atomicAdd(&a.done_cols[u], 1) == kCorrWarps * N2 - 1;
+        last = atomicAdd(&a.done_cols[u], 1) == F::kDone - 1;
     }
     *last_out = last;  // meaningful in lane 0 only
 }
@@ -272,21 +295,22 @@ __device__ __forceinline__ UnitOut unit_score(const UnitAcc& ac, int l) {
 
 // Thread 0 claims and resolves the dependency of the next item while the
 // CTA works on the current one; one barrier publishes it.
-template <int N2>
+template <int N2, int V>
 __device__ __forceinline__ void corr_wait_for(const CorrArgs& a, int item) {
-    const int s = item / (2 * N2), j = item - s * (2 * N2);
-    if (j < N2) {
-        if (s < a.nu && s >= a.S) wait_counter(a.done_cols + (s - a.S), kCorrWarps * N2, a.error);
+    using C = CorrCfg<N2, V>;
+    const int s = item / (2 * C::T), j = item - s * (2 * C::T);
+    if (j < C::T) {
+        if (s < a.nu && s >= a.S) wait_counter(a.done_cols + (s - a.S), C::kDone, a.error);
     } else {
         const int u = s - a.lag;
-        if (u >= 0 && u < a.nu) wait_counter(a.done_rows + u, kCorrWarps * N2, a.error);
+        if (u >= 0 && u < a.nu) wait_counter(a.done_rows + u, C::kDone, a.error);
     }
 }
 
-template <int N2>
-__global__ void __launch_bounds__(256, 2) k_corr_persistent(CorrArgs a) {
-    using F = Fast16<N2>;
-    using SM = CorrSmem<N2>;
+template <int N2, int V>
+__global__ void __launch_bounds__(CorrCfg<N2, V>::kThreads, CorrCfg<N2, V>::kCtasPerSm) k_corr_persistent(CorrArgs a) {
+    using F = CorrCfg<N2, V>;
+    using SM = CorrSmem<N2, V>;
     extern __shared__ __align__(16) unsigned char smc[];
     float2* tile = reinterpret_cast<float2*>(smc);
     float2* twt = reinterpret_cast<float2*>(smc + SM::tile);
@@ -298,10 +322,10 @@ __global__ void __launch_bounds__(256, 2) k_corr_persistent(CorrArgs a) {
         sincospi(2.0 * (double)((n2 * k1) % F::L) / (double)F::L, &sn, &cs);
         twt[i] = make_float2((float)cs, (float)sn);
     }
-    const int total = (a.nu + a.lag) * 2 * N2;
+    const int total = (a.nu + a.lag) * 2 * F::T;
     if (threadIdx.x == 0) {
         const int first = atomicAdd(a.next_item, 1);
-        if (first < total) corr_wait_for<N2>(a, first);
+        if (first < total) corr_wait_for<N2, V>(a, first);
         ish[0] = first;
     }
     __syncthreads();
@@ -309,16 +333,16 @@ __global__ void __launch_bounds__(256, 2) k_corr_persistent(CorrArgs a) {
     for (int iter = 1; item < total; ++iter) {
         int nxt = 0;
         if (threadIdx.x == 0) nxt = atomicAdd(a.next_item, 1);  // consumed after the tile
-        const int s = item / (2 * N2), j = item - s * (2 * N2);
-        if (j < N2) {
+        const int s = item / (2 * F::T), j = item - s * (2 * F::T);
+        if (j < F::T) {
             if (s < a.nu) {
-                corr_row_tile<N2>(a, s, j, tile, twt);
+                corr_row_tile<N2, V>(a, s, j, tile, twt);
             }
         } else {
             const int u = s - a.lag;
             if (u >= 0 && u < a.nu) {
                 bool last = false;
-                corr_col_tile<N2>(a, u, j - N2, tile, twt, &last);
+                corr_col_tile<N2, V>(a, u, j - F::T, tile, twt, &last);
                 if ((threadIdx.x & 31) == 0 && last) {
                     __threadfence();
                     const int2 wp = a.unit_wp[u];
@@ -336,7 +360,7 @@ __global__ void __launch_bounds__(256, 2) k_corr_persistent(CorrArgs a) {
             }
         }
         if (threadIdx.x == 0) {
-            if (nxt < total) corr_wait_for<N2>(a, nxt);
+            if (nxt < total) corr_wait_for<N2, V>(a, nxt);
             ish[iter & 3] = nxt;
         }
         // one barrier: the tile buffer is free again and the next item (with its

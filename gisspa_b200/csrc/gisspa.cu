@@ -40,7 +40,7 @@ struct DBuf {
 }  // namespace
 
 struct CorrTuningSaved {
-    int slots, lag, window_block, ctas;
+    int slots, lag, window_block, ctas, tile;
 };
 
 namespace {
@@ -72,11 +72,12 @@ struct gs_ctx {
     int window_block = 4;
     int corr_slots = 16, corr_lag = 6;
     int corr_ctas = 0;                 // resident CTAs per SM of the persistent kernels (0 = as many as fit)
+    int corr_tile = 16;                // vectors per tile of the FP32 persistent kernel (16 or 8)
     int corr_ctas_override = 0;        // value used by the launch in progress
     bool use_graph = false;            // capture the angle loop as one CUDA graph
     bool autotune = false;             // tune the persistent kernels' scheduling on first use
     std::map<long long, struct CorrTuningSaved> tuned;
-    int last_tuning[4] = {0, 0, 0, 0};
+    int last_tuning[5] = {0, 0, 0, 0, 0};
     unsigned long long graph_kernel_launches = 0;
     DBuf unit_wp, dep_counters, pacc, flags;
     // off-grid refinement (refine.cuh): per-pick chunk buffers
@@ -235,29 +236,33 @@ int run_fast(gs_ctx* ctx, int l, int nimg, IO io) {
     }
 }
 
-template <int N2>
-int launch_corr_n2(gs_ctx* ctx, const CorrArgs& a, long long total_items) {
-    const size_t smem = CorrSmem<N2>::bytes;
-    auto kern = k_corr_persistent<N2>;
+template <int N2, int V>
+int launch_corr_nv(gs_ctx* ctx, const CorrArgs& a) {
+    using C = CorrCfg<N2, V>;
+    const size_t smem = CorrSmem<N2, V>::bytes;
+    auto kern = k_corr_persistent<N2, V>;
     CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0, nsm = 0, dev = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, C::kThreads, smem));
     if (per_sm < 1) return set_err(ctx, GS_ERR_UNSUPPORTED, "persistent kernel does not fit on an SM");
     if (ctx->corr_ctas_override > 0) per_sm = std::min(per_sm, ctx->corr_ctas_override);
+    const long long total_items = (long long)(a.nu + a.lag) * 2 * C::T;
     const long long grid = std::min<long long>((long long)nsm * per_sm, total_items);
-    kern<<<(unsigned)grid, 256, smem, ctx->stream>>>(a);
+    kern<<<(unsigned)grid, C::kThreads, smem, ctx->stream>>>(a);
     ++ctx->counters.kernel_launches;
     CKL();
     return GS_OK;
 }
 
-int launch_corr(gs_ctx* ctx, int l, const CorrArgs& a, long long total_items) {
+// Persistent FP32 correlation with tiles of `tile` vectors (16 or 8).
+int launch_corr(gs_ctx* ctx, int l, int tile, const CorrArgs& a) {
+    const bool wide = tile != 8;
     switch (l / 16) {
-        case 32: return launch_corr_n2<32>(ctx, a, total_items);
-        case 45: return launch_corr_n2<45>(ctx, a, total_items);
-        case 48: return launch_corr_n2<48>(ctx, a, total_items);
+        case 32: return wide ? launch_corr_nv<32, 16>(ctx, a) : launch_corr_nv<32, 8>(ctx, a);
+        case 45: return wide ? launch_corr_nv<45, 16>(ctx, a) : launch_corr_nv<45, 8>(ctx, a);
+        case 48: return wide ? launch_corr_nv<48, 16>(ctx, a) : launch_corr_nv<48, 8>(ctx, a);
         default: return set_err(ctx, GS_ERR_UNSUPPORTED, "no persistent kernel for %d", l);
     }
 }
@@ -1079,7 +1084,7 @@ static int prep_micrograph(gs_ctx* ctx, const MicPlan& mp, float2* W) {
 // Scheduling of the persistent correlation: ring slots, lag, window block,
 // resident CTAs per SM (0 = as many as fit).
 struct CorrTuning {
-    int slots, lag, window_block, ctas;
+    int slots, lag, window_block, ctas, tile;
 };
 
 // Unit order: blocks of window_block windows; inside a block, pair-major.
@@ -1126,7 +1131,7 @@ static int corr_launch(gs_ctx* ctx, const float2* W, const float2* TS, int nu, c
         if (ca.yb1 < ca.yb0) { ca.yb0 = 1; ca.yb1 = 0; }
     }
     ctx->corr_ctas_override = t.ctas;
-    if (ctx->p.precision == GS_PREC_FP32) return launch_corr(ctx, l, ca, (long long)(nu + t.lag) * 2 * (l / 16));
+    if (ctx->p.precision == GS_PREC_FP32) return launch_corr(ctx, l, t.tile, ca);
     return launch_corr_tc(ctx, l, ctx->p.precision == GS_PREC_TC_BF16, ca);
 }
 
@@ -1140,13 +1145,15 @@ static int autotune(gs_ctx* ctx, const float2* W, const float2* TS, int NW, Corr
     const long long key = (((long long)ctx->l * 1000003 + N) * 1000003 + NW) * 4 + ctx->p.precision;
     auto it = ctx->tuned.find(key);
     if (it != ctx->tuned.end()) {
-        *best = CorrTuning{it->second.slots, it->second.lag, it->second.window_block, it->second.ctas};
+        *best = CorrTuning{it->second.slots, it->second.lag, it->second.window_block, it->second.ctas,
+                           it->second.tile};
         return GS_OK;
     }
     const int nu_full = Np * NW;
     const int nu = std::min(nu_full, 8192);
     std::vector<int> slots_c = {8, 12, 16, 24, 32}, lag_c = {2, 4, 6, 10}, wb_c = {1, 2, 4, 8}, ctas_c = {0, 1};
-    CorrTuning cur{ctx->corr_slots, ctx->corr_lag, ctx->window_block, 0};
+    std::vector<int> tile_c = {16, 8};
+    CorrTuning cur{ctx->corr_slots, ctx->corr_lag, ctx->window_block, 0, ctx->corr_tile};
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
@@ -1168,16 +1175,20 @@ static int autotune(gs_ctx* ctx, const float2* W, const float2* TS, int NW, Corr
     };
     float best_ms = 0;
     TRY(time_of(cur, &best_ms));
-    for (int pass = 0; pass < 4; ++pass) {
-        const std::vector<int>& cand = pass == 0 ? slots_c : pass == 1 ? lag_c : pass == 2 ? wb_c : ctas_c;
+    const int npass = ctx->p.precision == GS_PREC_FP32 ? 5 : 4;  // the tile width exists in the FP32 kernel only
+    for (int pass = 0; pass < npass; ++pass) {
+        const std::vector<int>& cand =
+            pass == 0 ? slots_c : pass == 1 ? lag_c : pass == 2 ? wb_c : pass == 3 ? ctas_c : tile_c;
         for (int v : cand) {
             CorrTuning t = cur;
             if (pass == 0) t.slots = v;
             else if (pass == 1) t.lag = v;
             else if (pass == 2) t.window_block = v;
-            else t.ctas = v;
+            else if (pass == 3) t.ctas = v;
+            else t.tile = v;
             if (t.lag >= t.slots) continue;
-            if (t.slots == cur.slots && t.lag == cur.lag && t.window_block == cur.window_block && t.ctas == cur.ctas)
+            if (t.slots == cur.slots && t.lag == cur.lag && t.window_block == cur.window_block &&
+                t.ctas == cur.ctas && t.tile == cur.tile)
                 continue;
             float ms = 0;
             TRY(time_of(t, &ms));
@@ -1190,7 +1201,7 @@ static int autotune(gs_ctx* ctx, const float2* W, const float2* TS, int NW, Corr
     int flag = 0;
     CK(cudaMemcpy(&flag, ctx->flags.p, sizeof(int), cudaMemcpyDeviceToHost));
     if (flag) return set_err(ctx, GS_ERR_TIMEOUT, "correlation kernel: a bounded dependency wait gave up (autotuner)");
-    ctx->tuned[key] = CorrTuningSaved{cur.slots, cur.lag, cur.window_block, cur.ctas};
+    ctx->tuned[key] = CorrTuningSaved{cur.slots, cur.lag, cur.window_block, cur.ctas, cur.tile};
     *best = cur;
     return GS_OK;
 }
@@ -1223,7 +1234,7 @@ static int correlate_all(gs_ctx* ctx, const float2* W, int NW, const std::vector
     UnitOut* units = P<UnitOut>(ctx->units);
     FftPlan* plan = nullptr;
     TRY(get_plan(ctx, l, &plan));  // before any capture: plan creation copies synchronously
-    CorrTuning tune{ctx->corr_slots, ctx->corr_lag, ctx->window_block, ctx->corr_ctas};
+    CorrTuning tune{ctx->corr_slots, ctx->corr_lag, ctx->window_block, ctx->corr_ctas, ctx->corr_tile};
     if (persistent) {
         TRY(ensure(ctx, ctx->dep_counters, sizeof(int) * (2 * (size_t)nu + 4)));
         TRY(ensure(ctx, ctx->pacc, sizeof(UnitAcc) * 2 * (size_t)nu));
@@ -1243,6 +1254,7 @@ static int correlate_all(gs_ctx* ctx, const float2* W, int NW, const std::vector
     ctx->last_tuning[1] = tune.lag;
     ctx->last_tuning[2] = tune.window_block;
     ctx->last_tuning[3] = tune.ctas;
+    ctx->last_tuning[4] = p.precision == GS_PREC_FP32 ? tune.tile : 8;
     float2* R = P<float2>(ctx->scratch);
     UnitAcc* acc = P<UnitAcc>(ctx->acc);
     const float q_lo = p.d_m / 4.0f;
@@ -1629,6 +1641,10 @@ int gs_set_option(gs_ctx* ctx, int option, int value) {
             ctx->corr_ctas = value;
             return GS_OK;
         case GS_OPT_GRAPH: ctx->use_graph = value != 0; return GS_OK;
+        case GS_OPT_CORR_TILE:
+            if (value != 8 && value != 16) return set_err(ctx, GS_ERR_ARG, "tile width must be 8 or 16");
+            ctx->corr_tile = value;
+            return GS_OK;
         case GS_OPT_AUTOTUNE: ctx->autotune = value != 0; return GS_OK;
         default: return set_err(ctx, GS_ERR_ARG, "unknown option %d", option);
     }
@@ -1652,9 +1668,9 @@ int gs_refine(gs_ctx* ctx, gs_refine_pick* picks, int n, int steps, gs_refine_re
     return refine_impl(ctx, picks, n, steps, out);
 }
 
-int gs_get_tuning(gs_ctx* ctx, int* out4) {
-    if (!ctx || !out4) return set_err(ctx, GS_ERR_ARG, "null pointer");
-    for (int i = 0; i < 4; ++i) out4[i] = ctx->last_tuning[i];
+int gs_get_tuning(gs_ctx* ctx, int* out, int n) {
+    if (!ctx || !out || n < 0) return set_err(ctx, GS_ERR_ARG, "null pointer or n < 0");
+    for (int i = 0; i < n && i < 5; ++i) out[i] = ctx->last_tuning[i];
     return GS_OK;
 }
 

@@ -256,9 +256,9 @@ int gs_merge_duplicates(int device, const gs_merge_item* items, size_t n, double
                         double euler_thres, unsigned char* keep);
 
 /* Scheduling the last search used for the persistent correlation (after
- * autotuning when GS_OPT_AUTOTUNE is on): out4 = {ring slots, lag, window
- * block, CTAs per SM (0 = as many as fit)}. */
-int gs_get_tuning(struct gs_ctx* ctx, int* out4);
+ * autotuning when GS_OPT_AUTOTUNE is on): the first min(n, 5) of {ring
+ * slots, lag, window block, CTAs per SM (0 = as many as fit), tile width}. */
+int gs_get_tuning(struct gs_ctx* ctx, int* out, int n);
 
 /* Enable (1) or disable (0) per-kernel event timing of the correlation
  * passes; it adds two events per launch. */
@@ -290,9 +290,13 @@ int gs_set_kernel_timing(struct gs_ctx* ctx, int enable);
 #define GS_OPT_GRAPH 7
 /* GS_OPT_AUTOTUNE: 1 = before the first search of a given (window,
  * templates, windows, precision), time candidate ring slots, lag, window
- * block and CTAs per SM on angle 0 over up to 8192 units and keep the
- * fastest for this context (gs_get_tuning shows the choice). */
+ * block, CTAs per SM and tile width on angle 0 over up to 8192 units and
+ * keep the fastest for this context (gs_get_tuning shows the choice). */
 #define GS_OPT_AUTOTUNE 8
+/* GS_OPT_CORR_TILE: vectors per tile of the FP32 persistent kernel: 16
+ * (256-thread CTAs, two per SM; default) or 8 (128-thread CTAs, four per
+ * SM).  The autotuner also tries both. */
+#define GS_OPT_CORR_TILE 9
 int gs_set_option(struct gs_ctx* ctx, int option, int value);
 
 /* Counters of this context since creation (no reference counterpart; the

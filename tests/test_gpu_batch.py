@@ -89,18 +89,34 @@ def test_autotuned_equals_default(data):
     with G.Context(0) as ctx:
         ctx.set_templates(_params(), tmpl, ctf)
         ref = ctx.search(img, ctf)
-        assert ctx.tuning() == (16, 6, 4, 0)
+        assert ctx.tuning() == (16, 6, 4, 0, 16)
     with G.Context(0) as ctx:
         ctx.set_autotune(True)
         ctx.set_templates(_params(), tmpl, ctf)
         got = ctx.search(img, ctf)
-        slots, lag, wb, ctas = ctx.tuning()
+        slots, lag, wb, ctas, tile = ctx.tuning()
         again = ctx.search(img, ctf)          # cached choice
-        assert ctx.tuning() == (slots, lag, wb, ctas)
-    print("autotuned scheduling: slots %d lag %d window block %d ctas/SM %d" % (slots, lag, wb, ctas))
-    assert 0 <= lag < slots and wb >= 1 and ctas >= 0
+        assert ctx.tuning() == (slots, lag, wb, ctas, tile)
+    print("autotuned scheduling: slots %d lag %d window block %d ctas/SM %d tile %d"
+          % (slots, lag, wb, ctas, tile))
+    assert 0 <= lag < slots and wb >= 1 and ctas >= 0 and tile in (8, 16)
     _same(got, ref)
     _same(again, ref)
+
+
+def test_narrow_tiles_equal_wide(data):
+    """The persistent kernel with 8-vector tiles (four 128-thread CTAs per
+    SM) against the default 16-vector tiles."""
+    tmpl, mics = data
+    res = []
+    for tile in (16, 8):
+        with G.Context(0) as ctx:
+            ctx.set_corr_tile(tile)
+            ctx.set_templates(_params(), tmpl, mics[0][1])
+            res.append(ctx.search_batch([m[0] for m in mics], [m[1] for m in mics]))
+            assert ctx.tuning()[4] == tile
+    for a, b in zip(*res):
+        _same(a, b)
 
 
 def test_two_pass_batch(data):
