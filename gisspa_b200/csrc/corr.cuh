@@ -25,9 +25,9 @@
 // still completes and signals, so no other CTA is left waiting on it.
 //
 // Memory ordering: producers store the maps bypassing L1 (st.global with an
-// L2 cache hint), then
-// __syncwarp(), and lane 0 of each warp issues __threadfence() + atomicAdd on
-// the unit's counter; the consumer CTA's thread 0 spins with ld.acquire.gpu
+// L2 cache hint), then __syncwarp(), and lane 0 of each warp increments the
+// unit's counter with a release reduction (the column tiles' accumulator
+// atomics are followed by an acquire-release add); the consumer CTA's thread 0 spins with ld.acquire.gpu
 // and fences before the CTA barrier that publishes the item, and its threads
 // read the maps with L1::no_allocate loads (L2, never a stale L1 line from an
 // earlier occupant of the slot).  Each item costs two CTA barriers: step 1 -> step 2
@@ -176,11 +176,11 @@ __device__ __forceinline__ void corr_row_tile(const CorrArgs& a, int u, int t, f
         });
     }
     // publish this warp's share of the tile
+    // (release: the warp's map stores, ordered by __syncwarp, become visible
+    // before the count; cheaper than a full fence + atomic)
     __syncwarp();
-    if ((threadIdx.x & 31) == 0) {
-        __threadfence();
-        atomicAdd(&a.done_rows[u], 1);
-    }
+    if ((threadIdx.x & 31) == 0)
+        asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(&a.done_rows[u]) : "memory");
 }
 
 template <int N2, int V>
@@ -272,8 +272,9 @@ __device__ __forceinline__ void corr_col_tile(const CorrArgs& a, int u, int t, f
         if (kb) atomicMax(&ac[1].key, kb);
         atomicAdd(&ac[1].s1, d1b);
         atomicAdd(&ac[1].s2, d2b);
-        __threadfence();
-        last = atomicAdd(&a.done_cols[u], 1) == F::kDone - 1;
+        int prev;
+        asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;" : "=r"(prev) : "l"(&a.done_cols[u]) : "memory");
+        last = prev == F::kDone - 1;
     }
     *last_out = last;  // meaningful in lane 0 only
 }
