@@ -6,7 +6,8 @@
 // with T = l / V tiles of V vectors (V = 16 or 8, CorrCfg).  A row tile takes V
 // spectrum rows of unit u: S = W_w conj(P_p), inverse FFT along x (the
 // four-step l = 16 N2 transform of fastfft.cuh), written to scratch map slot
-// u % S.  A column tile takes V columns of that map: inverse FFT along y and the score
+// u % S (for odd N2 prime-factor transforms along both axes, CorrCfg::kPfa).
+// A column tile takes V columns of that map: inverse FFT along y and the score
 // epilogue (border-masked peak and position, sum and sum of squares of both
 // templates of the pair), reduced into the unit's accumulators; the last
 // column tile of a unit computes the two scores.
@@ -76,6 +77,13 @@ __device__ __forceinline__ void wait_counter(const int* p, int target, int* erro
     atomicExch(error, 1);
 }
 
+// b^-1 mod m for gcd(b, m) = 1 (compile time, m small)
+constexpr int inv_mod(int b, int m) {
+    for (int x = 1; x < m; ++x)
+        if ((b * x) % m == 1) return x;
+    return m == 1 ? 0 : -1;
+}
+
 // Tile geometry: V vectors per tile (16 or 8), 16 V threads per CTA (step 2
 // has one (vector, k1) task per thread), 512 / (16 V) CTAs per SM.  A pass of
 // one unit is T = L / V tiles and kDone = (warps per CTA) x T per-warp
@@ -92,13 +100,37 @@ struct CorrCfg {
     static constexpr int kDone = kWarps * T;
     static constexpr int kCtasPerSm = 512 / kThreads;
     static_assert(V == 8 || V == 16, "tile width");
+    // Odd N2 (l = 720 = 16 x 45): 16 and N2 are coprime, so both passes use
+    // the Good-Thomas mapping and need no twiddles between their two DFT
+    // steps.  Along x the spectra arrive in that mapping's input order
+    // (PfaCols: physical column n2 + N2 n1 holds frequency (N2 n1 + 16 n2)
+    // mod L).  Along y the column pass's input row n2 + N2 n1 must hold
+    // spectrum row (N2 n1 + 16 n2) mod L, so the row pass reads the spectrum
+    // rows in that order.  Either pass's output k1 + 16 k2 is map coordinate
+    // (A1 k1 + A2 k2) mod L, A1 = 1 mod 16, 0 mod N2 and A2 = 0 mod 16, 1 mod N2.
+    static constexpr bool kPfa = (N2 % 2) == 1;
+    static constexpr int A1 = kPfa ? (N2 * inv_mod(N2 % 16, 16)) % L : 1;
+    static constexpr int A2 = kPfa ? (16 * inv_mod(16 % N2, N2)) % L : 16;
+    // spectrum row that physical row r of the scratch map holds
+    __device__ __forceinline__ static int spectrum_row(int r) {
+        if constexpr (kPfa) {
+            const int n1 = r / N2, n2 = r - n1 * N2;
+            const int q = N2 * n1 + 16 * n2;
+            return q < L ? q : q - L;  // N2 n1 + 16 n2 < 2 L
+        } else {
+            return r;
+        }
+    }
+    // map coordinate of pass output (k1, k2): x of physical column k1 + 16 k2,
+    // y of column-pass output k2 of thread k1
+    __host__ __device__ static constexpr int map_coord(int k1, int k2) { return (A1 * k1 + A2 * k2) % L; }
 };
 
 template <int N2, int V>
 struct CorrSmem {
     using C = CorrCfg<N2, V>;
     static constexpr size_t tile = (size_t)C::V * C::VP * sizeof(float2);
-    static constexpr size_t tw = (size_t)16 * N2 * sizeof(float2);
+    static constexpr size_t tw = C::kPfa ? 0 : (size_t)16 * N2 * sizeof(float2);  // no twiddles with kPfa
     static constexpr size_t red = 128 * sizeof(double);
     static constexpr size_t bytes = tile + tw + red + 32;
 };
@@ -147,7 +179,7 @@ __device__ __forceinline__ void corr_row_tile(const CorrArgs& a, int u, int t, f
     const unsigned long long keep = l2_policy_evict_last();
     for (int task = threadIdx.x; task < F::V * N2; task += F::kThreads) {
         const int v = task / N2, n2 = task - v * N2;
-        const long long base = (long long)(r0 + v) * L + n2;
+        const long long base = (long long)F::spectrum_row(r0 + v) * L + n2;
         float2 x[16];
 #pragma unroll
         for (int n1 = 0; n1 < 16; ++n1)
@@ -158,7 +190,7 @@ __device__ __forceinline__ void corr_row_tile(const CorrArgs& a, int u, int t, f
         rf::static_for<16>([&](auto kc) {
             constexpr int k1 = decltype(kc)::value;
             constexpr int r = rf::rpos<16>(k1);
-            dst[k1 * F::BP] = k1 ? cmul(x[r], tw[k1 * N2]) : x[r];
+            dst[k1 * F::BP] = (k1 && !F::kPfa) ? cmul(x[r], tw[k1 * N2]) : x[r];
         });
     }
     __syncthreads();
@@ -183,9 +215,27 @@ __device__ __forceinline__ void corr_row_tile(const CorrArgs& a, int u, int t, f
         asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(&a.done_rows[u]) : "memory");
 }
 
+// Border mask of the map rows one column-pass thread produces: bit k2 is set
+// when map row map_coord(k1, k2) lies outside the border interval [yb0, yb1]
+// (the thread's k1 is fixed for the life of the kernel).
+template <int N2, int V>
+__device__ __forceinline__ uint2 corr_row_mask(int yb0, int yb1) {
+    using F = CorrCfg<N2, V>;
+    const int k1 = V == 16 ? (threadIdx.x >> 4) : (threadIdx.x & 15);
+    uint2 m = make_uint2(0u, 0u);
+    for (int k2 = 0; k2 < N2; ++k2) {
+        const int y = F::map_coord(k1, k2);
+        if ((unsigned)(y - yb0) > (unsigned)(yb1 - yb0)) {
+            if (k2 < 32) m.x |= 1u << k2;
+            else m.y |= 1u << (k2 - 32);
+        }
+    }
+    return m;
+}
+
 template <int N2, int V>
 __device__ __forceinline__ void corr_col_tile(const CorrArgs& a, int u, int t, float2* tile, const float2* twt,
-                                              bool* last_out) {
+                                              uint2 ymask, bool* last_out) {
     using F = CorrCfg<N2, V>;
     constexpr int L = F::L;
     constexpr int h = L / 2;
@@ -204,7 +254,7 @@ __device__ __forceinline__ void corr_col_tile(const CorrArgs& a, int u, int t, f
         rf::static_for<16>([&](auto kc) {
             constexpr int k1 = decltype(kc)::value;
             constexpr int r = rf::rpos<16>(k1);
-            dst[k1 * F::BP] = k1 ? cmul(x[r], tw[k1 * N2]) : x[r];
+            dst[k1 * F::BP] = (k1 && !F::kPfa) ? cmul(x[r], tw[k1 * N2]) : x[r];
         });
     }
     __syncthreads();
@@ -218,8 +268,10 @@ __device__ __forceinline__ void corr_col_tile(const CorrArgs& a, int u, int t, f
     // for their width
     const int v = V == 16 ? (threadIdx.x & 15) : (threadIdx.x >> 4);
     const int k1 = V == 16 ? (threadIdx.x >> 4) : (threadIdx.x & 15);
-    const int x = c0 + v;
-    const bool xin = (unsigned)(x - a.yb0) > (unsigned)(a.yb1 - a.yb0);  // column outside the border
+    // map column held by physical column c0 + v (the row pass's output order)
+    const int x = F::kPfa ? F::map_coord((c0 + v) & 15, (c0 + v) >> 4) : c0 + v;
+    // column outside the border: the rows of ymask count, else none
+    if ((unsigned)(x - a.yb0) <= (unsigned)(a.yb1 - a.yb0)) ymask = make_uint2(0u, 0u);
     float best1 = 0.0f, best2 = 0.0f;   // reference peak = max(0, masked max)
     int bk1 = -1, bk2 = -1;
     float s1a = 0.f, s2a = 0.f, s1b = 0.f, s2b = 0.f;
@@ -232,8 +284,7 @@ __device__ __forceinline__ void corr_col_tile(const CorrArgs& a, int u, int t, f
         rf::static_for<N2>([&](auto kc) {
             constexpr int k2 = decltype(kc)::value;
             const float2 val = b[rf::rpos<N2>(k2)];
-            const int y = k1 + 16 * k2;
-            const bool in = xin && ((unsigned)(y - a.yb0) > (unsigned)(a.yb1 - a.yb0));
+            const bool in = (((k2 < 32 ? ymask.x : ymask.y) >> (k2 & 31)) & 1u) != 0u;
             const float v1 = ((L / 2) % 2 == 0) ? val.x : -val.x;
             const float v2 = ((L / 2) % 2 == 0) ? val.y : -val.y;
             const bool g1 = in && v1 > best1, g2 = in && v2 > best2;
@@ -245,16 +296,17 @@ __device__ __forceinline__ void corr_col_tile(const CorrArgs& a, int u, int t, f
             s1b += v2; s2b = fmaf(v2, v2, s2b);
         });
     }
-    // keys: value bits high, ~flat index low (smallest index wins among equal values)
+    // keys: value bits high, ~flat index low (among equal values the smallest
+    // index wins across threads; within one thread, the first in k2 order)
     const int X = x + h < L ? x + h : x - h;
     unsigned long long ka = 0ull, kb = 0ull;
     if (bk1 >= 0) {
-        const int y = k1 + 16 * bk1;
+        const int y = F::map_coord(k1, bk1);
         const int Y = y + h < L ? y + h : y - h;
         ka = argmax_key(best1, Y * L + X);
     }
     if (bk2 >= 0) {
-        const int y = k1 + 16 * bk2;
+        const int y = F::map_coord(k1, bk2);
         const int Y = y + h < L ? y + h : y - h;
         kb = argmax_key(best2, Y * L + X);
     }
@@ -317,12 +369,13 @@ __global__ void __launch_bounds__(CorrCfg<N2, V>::kThreads, CorrCfg<N2, V>::kCta
     float2* twt = reinterpret_cast<float2*>(smc + SM::tile);
     int* ish = reinterpret_cast<int*>(smc + SM::tile + SM::tw + SM::red);  // ring of 4 broadcast slots
     // inverse twiddles W_L^{-n2 k1} = exp(+2 pi i n2 k1 / L), table [k1][n2]
-    for (int i = threadIdx.x; i < 16 * N2; i += F::kThreads) {
+    for (int i = threadIdx.x; i < (F::kPfa ? 0 : 16 * N2); i += F::kThreads) {
         const int k1 = i / N2, n2 = i - k1 * N2;
         double sn, cs;
         sincospi(2.0 * (double)((n2 * k1) % F::L) / (double)F::L, &sn, &cs);
         twt[i] = make_float2((float)cs, (float)sn);
     }
+    const uint2 ymask = corr_row_mask<N2, V>(a.yb0, a.yb1);
     const int total = (a.nu + a.lag) * 2 * F::T;
     if (threadIdx.x == 0) {
         const int first = atomicAdd(a.next_item, 1);
@@ -343,7 +396,7 @@ __global__ void __launch_bounds__(CorrCfg<N2, V>::kThreads, CorrCfg<N2, V>::kCta
             const int u = s - a.lag;
             if (u >= 0 && u < a.nu) {
                 bool last = false;
-                corr_col_tile<N2, V>(a, u, j - F::T, tile, twt, &last);
+                corr_col_tile<N2, V>(a, u, j - F::T, tile, twt, ymask, &last);
                 if ((threadIdx.x & 31) == 0 && last) {
                     __threadfence();
                     const int2 wp = a.unit_wp[u];

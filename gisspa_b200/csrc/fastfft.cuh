@@ -95,6 +95,56 @@ __global__ void __launch_bounds__(256, 2) k_fft16(const float2* __restrict__ tw,
 
 // ---- IO functors: (img, v, k) -> element k of vector v of image img ----
 
+// Column order of spectra fed to a prime-factor inverse transform along x
+// (L = 16 N2, N2 odd, so 16 and N2 are coprime): physical column
+// p = n2 + N2 n1 holds frequency (N2 n1 + 16 n2) mod L, the Good-Thomas input
+// map, so that the transform reads its 16-point groups at stride N2 exactly
+// like the four-step kernels.  N2 = 0 means natural order.
+struct PfaCols {
+    int L = 0, N2 = 0;
+    int i16 = 0;  // N2^-1 mod 16
+    int iN = 0;   // 16^-1 mod N2
+    static PfaCols make(int l) {
+        PfaCols c;
+        if (l % 16 || (l / 16) % 2 == 0) return c;
+        c.L = l;
+        c.N2 = l / 16;
+        for (int x = 1; x < 16; ++x)
+            if ((c.N2 * x) % 16 == 1) c.i16 = x;
+        for (int x = 1; x < c.N2; ++x)
+            if ((16 * x) % c.N2 == 1) c.iN = x;
+        return c;
+    }
+    // frequency held by physical column p
+    __host__ __device__ int logical(int p) const {
+        const int n1 = p / N2, n2 = p - n1 * N2;
+        const int q = N2 * n1 + 16 * n2;
+        return q < L ? q : q - L;
+    }
+    // physical column of frequency k = k1 + 16 k2: n1 = k1 / N2 mod 16,
+    // n2 = k / 16 mod N2 = k1 iN + k2 mod N2
+    __host__ __device__ int physical(int k) const {
+        const int k1 = k & 15;
+        const int n1 = (k1 * i16) & 15;
+        const int n2 = (k1 * iN + (k >> 4)) % N2;
+        return n2 + N2 * n1;
+    }
+};
+
+// In place, every row of `rows` rows of length L: to_physical moves
+// natural-order columns to the PfaCols order, otherwise back.
+__global__ void k_pfa_permute_rows(float2* __restrict__ data, long long rows, PfaCols pc, bool to_physical) {
+    extern __shared__ float2 prow[];
+    const int L = pc.L;
+    for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
+        float2* row = data + r * L;
+        for (int i = threadIdx.x; i < L; i += blockDim.x) prow[i] = row[i];
+        __syncthreads();
+        for (int i = threadIdx.x; i < L; i += blockDim.x) row[i] = prow[to_physical ? pc.logical(i) : pc.physical(i)];
+        __syncthreads();
+    }
+}
+
 template <bool kCols>
 __device__ __forceinline__ long long f16_addr(int L, long long L2, int img, int v, int k) {
     return (long long)img * L2 + (kCols ? (long long)k * L + v : (long long)v * L + k);
@@ -147,12 +197,15 @@ struct F16PairNorm {
     const float4* coef;
     int L;
     long long L2;
+    PfaCols pfa;  // pfa.N2 != 0: store the row spectra in prime-factor column order
     __device__ float2 load(int img, int v, int k) const {
         const float4 c = coef[img];
         const float2 z = data[f16_addr<false>(L, L2, img, v, k)];
         return make_float2((z.x - c.x) * c.y, -(z.y - c.z) * c.w);
     }
-    __device__ void store(int img, int v, int k, float2 x) const { data[f16_addr<false>(L, L2, img, v, k)] = x; }
+    __device__ void store(int img, int v, int k, float2 x) const {
+        data[f16_addr<false>(L, L2, img, v, pfa.N2 ? pfa.physical(k) : k)] = x;
+    }
     __device__ void finish(double*) const {}
 };
 

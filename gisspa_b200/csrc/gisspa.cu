@@ -370,7 +370,9 @@ unsigned blocks_for(long long n, int threads, unsigned cap = 1u << 30) {
 // Template-pair spectra of one in-plane angle (rotate_template + the
 // normalisation and FFT of main.cu:1236-1249): TS[p] = FFT(t_2p - i t_2p+1) / l^2
 // with each rotated, masked template mean/variance normalised.
-static int pair_spectra(gs_ctx* ctx, float e, float2* TS) {
+// pfa: store the spectra in the PfaCols column order of the prime-factor
+// correlation kernel (window 720) instead of natural order.
+static int pair_spectra(gs_ctx* ctx, float e, float2* TS, bool pfa = false) {
     const int l = ctx->l, N = ctx->ntmpl, Np = (N + 1) / 2;
     const long long l2 = (long long)l * l;
     const double ang = (double)e * kPiRef / 180.0;
@@ -384,7 +386,7 @@ static int pair_spectra(gs_ctx* ctx, float e, float2* TS) {
     ++ctx->counters.kernel_launches;
     CKL();
     if (fast_ok(ctx, l)) {
-        TRY(run_fast<false, false>(ctx, l, Np, F16PairNorm{TS, P<float4>(ctx->coef), l, l2}));
+        TRY(run_fast<false, false>(ctx, l, Np, F16PairNorm{TS, P<float4>(ctx->coef), l, l2, pfa ? PfaCols::make(l) : PfaCols{}}));
         TRY(run_fast<false, true>(ctx, l, Np, F16Complex<true>{TS, l, l2, (float)(1.0 / (double)l2)}));
     } else {
         TRY(run_fft<false>(ctx, l, rows_of(l, l), Np, IoPairNorm{TS, P<float4>(ctx->coef), l2}));
@@ -1210,7 +1212,7 @@ static int autotune(gs_ctx* ctx, const float2* W, const float2* TS, int NW, Corr
 // angle loop of main.cu:1232-1257): per angle the template-pair spectra, then
 // either one persistent launch over all (window, pair) units or per-window
 // row and column launches.  Results to ctx->units [angle][NW][N].
-static int correlate_all(gs_ctx* ctx, const float2* W, int NW, const std::vector<float>& angles, float* t_spec,
+static int correlate_all(gs_ctx* ctx, float2* W, int NW, const std::vector<float>& angles, float* t_spec,
                          float* t_corr, float kt[4]) {
     const gs_params& p = ctx->p;
     const int l = ctx->l;
@@ -1219,6 +1221,9 @@ static int correlate_all(gs_ctx* ctx, const float2* W, int NW, const std::vector
     const int na = (int)angles.size();
     const long long total_units = (long long)na * NW * N;
     const bool persistent = fast_ok(ctx, l) && !ctx->two_pass;
+    // the FP32 persistent kernel at window 720 takes prime-factor transforms
+    // and reads its spectra in PfaCols column order
+    const bool pfa = persistent && p.precision == GS_PREC_FP32 && PfaCols::make(l).N2 != 0;
     if (p.precision != GS_PREC_FP32 && !persistent)
         return set_err(ctx, GS_ERR_UNSUPPORTED,
                        "tensor-core precision needs window 512, 720 or 768 and the persistent path (window %d)", l);
@@ -1235,6 +1240,27 @@ static int correlate_all(gs_ctx* ctx, const float2* W, int NW, const std::vector
     FftPlan* plan = nullptr;
     TRY(get_plan(ctx, l, &plan));  // before any capture: plan creation copies synchronously
     CorrTuning tune{ctx->corr_slots, ctx->corr_lag, ctx->window_block, ctx->corr_ctas, ctx->corr_tile};
+    // window spectra in PfaCols order for the duration of the correlation,
+    // natural order again afterwards (on every return path)
+    struct PfaWindows {
+        gs_ctx* ctx;
+        float2* W;
+        long long rows;
+        PfaCols pc;
+        bool on = false;
+        int set(bool to_physical) {
+            const int threads = 256, blocks = (int)std::min<long long>(rows, 148 * 8);
+            k_pfa_permute_rows<<<blocks, threads, sizeof(float2) * pc.L, ctx->stream>>>(W, rows, pc, to_physical);
+            ++ctx->counters.kernel_launches;
+            if (cudaGetLastError() != cudaSuccess) return set_err(ctx, GS_ERR_CUDA, "k_pfa_permute_rows");
+            on = to_physical;
+            return GS_OK;
+        }
+        ~PfaWindows() {
+            if (on) set(false);
+        }
+    } pfa_w{ctx, W, (long long)NW * l, PfaCols::make(l)};
+    if (pfa) TRY(pfa_w.set(true));
     if (persistent) {
         TRY(ensure(ctx, ctx->dep_counters, sizeof(int) * (2 * (size_t)nu + 4)));
         TRY(ensure(ctx, ctx->pacc, sizeof(UnitAcc) * 2 * (size_t)nu));
@@ -1242,7 +1268,7 @@ static int correlate_all(gs_ctx* ctx, const float2* W, int NW, const std::vector
         CK(cudaMemsetAsync(ctx->flags.p, 0, sizeof(int) * 4, ctx->stream));
         if (ctx->autotune) {
             TRY(ensure(ctx, ctx->scratch, sizeof(float2) * l2 * 32));
-            TRY(pair_spectra(ctx, angles[0], TS));
+            TRY(pair_spectra(ctx, angles[0], TS, pfa));
             TRY(autotune(ctx, W, TS, NW, &tune));
         }
         TRY(upload_unit_order(ctx, NW, Np, tune.window_block, nu));
@@ -1279,7 +1305,7 @@ static int correlate_all(gs_ctx* ctx, const float2* W, int NW, const std::vector
     // the work of one angle, enqueued on the context's stream
     auto enqueue_angle = [&](int ai, bool rec) -> int {
         if (rec) CK(cudaEventRecord(ea, ctx->stream));
-        TRY(pair_spectra(ctx, angles[ai], TS));
+        TRY(pair_spectra(ctx, angles[ai], TS, pfa));
         if (rec) CK(cudaEventRecord(eb, ctx->stream));
         if (persistent) {
             if (timing) CK(cudaEventRecord(ctx->kev[0], ctx->stream));
