@@ -8,9 +8,10 @@
 // four-step l = 16 N2 transform of fastfft.cuh), written to scratch map slot
 // u % S (for odd N2 prime-factor transforms along both axes, CorrCfg::kPfa).
 // A column tile takes V columns of that map: inverse FFT along y and the score
-// epilogue (border-masked peak and position, sum and sum of squares of both
+// epilogue (border-masked peak and its position, sum of squares, for both
 // templates of the pair), reduced into the unit's accumulators; the last
-// column tile of a unit computes the two scores.
+// column tile of a unit computes the two scores, taking the maps' plain sums
+// from the spectrum's DC term (sum of the map = L^2 S(0, 0)).
 //
 // Dependencies and why they cannot deadlock: a column tile of u waits until
 // all T row tiles of u are done; a row tile of u >= S waits until all
@@ -272,9 +273,13 @@ __device__ __forceinline__ void corr_col_tile(const CorrArgs& a, int u, int t, f
     const int x = F::kPfa ? F::map_coord((c0 + v) & 15, (c0 + v) >> 4) : c0 + v;
     // column outside the border: the rows of ymask count, else none
     if ((unsigned)(x - a.yb0) <= (unsigned)(a.yb1 - a.yb0)) ymask = make_uint2(0u, 0u);
+    constexpr float sgn = ((L / 2) % 2 == 0) ? 1.0f : -1.0f;
+    // Per point the border-masked maximum with its k2 and the sum of squares;
+    // the map's plain sum is L^2 times its spectrum's DC term, taken when the
+    // unit's scores are computed.
     float best1 = 0.0f, best2 = 0.0f;   // reference peak = max(0, masked max)
     int bk1 = -1, bk2 = -1;
-    float s1a = 0.f, s2a = 0.f, s1b = 0.f, s2b = 0.f;
+    float s2a = 0.f, s2b = 0.f;
     {
         float2 b[N2];
         const float2* src = tile + v * F::VP + k1 * F::BP;
@@ -285,15 +290,14 @@ __device__ __forceinline__ void corr_col_tile(const CorrArgs& a, int u, int t, f
             constexpr int k2 = decltype(kc)::value;
             const float2 val = b[rf::rpos<N2>(k2)];
             const bool in = (((k2 < 32 ? ymask.x : ymask.y) >> (k2 & 31)) & 1u) != 0u;
-            const float v1 = ((L / 2) % 2 == 0) ? val.x : -val.x;
-            const float v2 = ((L / 2) % 2 == 0) ? val.y : -val.y;
+            const float v1 = sgn * val.x, v2 = sgn * val.y;
             const bool g1 = in && v1 > best1, g2 = in && v2 > best2;
             best1 = g1 ? v1 : best1;
             bk1 = g1 ? k2 : bk1;
             best2 = g2 ? v2 : best2;
             bk2 = g2 ? k2 : bk2;
-            s1a += v1; s2a = fmaf(v1, v1, s2a);
-            s1b += v2; s2b = fmaf(v2, v2, s2b);
+            s2a = fmaf(v1, v1, s2a);
+            s2b = fmaf(v2, v2, s2b);
         });
     }
     // keys: value bits high, ~flat index low (among equal values the smallest
@@ -310,19 +314,17 @@ __device__ __forceinline__ void corr_col_tile(const CorrArgs& a, int u, int t, f
         const int Y = y + h < L ? y + h : y - h;
         kb = argmax_key(best2, Y * L + X);
     }
-    // warp-level reduction, then one set of atomics per warp (no CTA barrier)
-    double d1a = warp_sum((double)s1a), d2a = warp_sum((double)s2a);
-    double d1b = warp_sum((double)s1b), d2b = warp_sum((double)s2b);
+    // warp-level reduction
+    const double d2a = warp_sum((double)s2a), d2b = warp_sum((double)s2b);
     ka = warp_max_u64(ka);
     kb = warp_max_u64(kb);
+    // one set of atomics per warp (no CTA barrier)
     bool last = false;
     if ((threadIdx.x & 31) == 0) {
         UnitAcc* ac = a.acc + 2 * (long long)u;
         if (ka) atomicMax(&ac[0].key, ka);
-        atomicAdd(&ac[0].s1, d1a);
         atomicAdd(&ac[0].s2, d2a);
         if (kb) atomicMax(&ac[1].key, kb);
-        atomicAdd(&ac[1].s1, d1b);
         atomicAdd(&ac[1].s2, d2b);
         int prev;
         asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;" : "=r"(prev) : "l"(&a.done_cols[u]) : "memory");
@@ -331,13 +333,14 @@ __device__ __forceinline__ void corr_col_tile(const CorrArgs& a, int u, int t, f
     *last_out = last;  // meaningful in lane 0 only
 }
 
-// Score of one template from its accumulators (main.cu:869-876).
-__device__ __forceinline__ UnitOut unit_score(const UnitAcc& ac, int l) {
+// Score of one template from its accumulators (main.cu:869-876); s1 is the
+// sum of the whole map.
+__device__ __forceinline__ UnitOut unit_score(const UnitAcc& ac, double s1, int l) {
     const float peak = key_value(ac.key);
     UnitOut u;
     u.peak = peak;
     u.pos = key_index(ac.key);
-    const double ra = ac.s1 - peak;
+    const double ra = s1 - peak;
     const double rb = ac.s2 - (double)peak * peak;
     const double rc = (double)l * l - 1.0;
     const double sd = sqrt(rb / rc - (ra / rc) * (ra / rc));
@@ -345,6 +348,7 @@ __device__ __forceinline__ UnitOut unit_score(const UnitAcc& ac, int l) {
     u.score = sd > 0.0 ? (float)(peak / sd) : __int_as_float(0x7fc00000);
     return u;
 }
+__device__ __forceinline__ UnitOut unit_score(const UnitAcc& ac, int l) { return unit_score(ac, ac.s1, l); }
 
 // Thread 0 claims and resolves the dependency of the next item while the
 // CTA works on the current one; one barrier publishes it.
@@ -401,14 +405,21 @@ __global__ void __launch_bounds__(CorrCfg<N2, V>::kThreads, CorrCfg<N2, V>::kCta
                     __threadfence();
                     const int2 wp = a.unit_wp[u];
                     const UnitAcc* ac = a.acc + 2 * (long long)u;
+                    // sum of the map c1 + i c2 = L^2 S(0, 0), S = W conj(P)
+                    // (frequency (0, 0) sits at element 0 in either column order)
+                    const float2 w0 = __ldg(a.W + (long long)wp.x * a.L2);
+                    const float2 p0 = __ldg(a.P + (long long)wp.y * a.L2);
+                    const double sg = ((F::L / 2) % 2 == 0) ? 1.0 : -1.0;
+                    const double l2 = (double)a.L2;
+                    const double sums[2] = {sg * l2 * ((double)w0.x * p0.x + (double)w0.y * p0.y),
+                                            sg * l2 * ((double)w0.y * p0.x - (double)w0.x * p0.y)};
                     for (int q = 0; q < 2; ++q) {
                         const int J = 2 * wp.y + q;
                         if (J >= a.ntmpl) break;
                         UnitAcc v;
                         v.key = __ldcg(&ac[q].key);
-                        v.s1 = __ldcg(&ac[q].s1);
                         v.s2 = __ldcg(&ac[q].s2);
-                        a.out[(long long)wp.x * a.ntmpl + J] = unit_score(v, F::L);
+                        a.out[(long long)wp.x * a.ntmpl + J] = unit_score(v, sums[q], F::L);
                     }
                 }
             }
