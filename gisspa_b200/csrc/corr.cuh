@@ -16,24 +16,28 @@
 // Dependencies and why they cannot deadlock: a column tile of u waits until
 // all T row tiles of u are done; a row tile of u >= S waits until all
 // column tiles of u - S are done (its scratch slot is free).  Completion is
-// counted per warp (every warp of a tile fences its own stores or atomics and
-// increments the unit's counter), so a pass of a unit is done at
-// (warps per CTA) x T increments and no CTA-wide barrier is needed to
-// publish a tile.  Both wait only
-// on items that come earlier in the claim order, and an item is claimed only
-// by a running CTA that finishes it before claiming another, so the earliest
-// unfinished item can always proceed.  Every wait is bounded; a wait that
-// gives up raises the error flag (reported as GS_ERR_TIMEOUT) and the item
-// still completes and signals, so no other CTA is left waiting on it.
+// counted per tile: after the CTA barrier that ends a tile, one thread (the
+// publisher, the CTA's last thread, which has the lightest share of step 1
+// when the tasks do not divide evenly) increments the unit's counter, so a
+// pass of a unit is done at T increments.  Each warp checks the dependency of
+// its CTA's next item itself before starting it.  Both dependencies point at
+// items that come earlier in the claim order, and an item is claimed only by
+// a running CTA that finishes and publishes it before it waits for anything
+// later, so the earliest unpublished item can always proceed.  Every wait is
+// bounded; a wait that gives up raises the error flag (reported as
+// GS_ERR_TIMEOUT) and the item still completes and is published, so no other
+// CTA is left waiting on it.
 //
 // Memory ordering: producers store the maps bypassing L1 (st.global with an
-// L2 cache hint), then __syncwarp(), and lane 0 of each warp increments the
-// unit's counter with a release reduction (the column tiles' accumulator
-// atomics are followed by an acquire-release add); the consumer CTA's thread 0 spins with ld.acquire.gpu
-// and fences before the CTA barrier that publishes the item, and its threads
-// read the maps with L1::no_allocate loads (L2, never a stale L1 line from an
-// earlier occupant of the slot).  Each item costs two CTA barriers: step 1 -> step 2
-// of the FFT, and the end-of-item barrier that hands over the next item.
+// L2 cache hint) and add their accumulator atomics; the CTA barrier that ends
+// the tile orders every thread's stores before the publisher's release
+// increment (acquire-release for column tiles, whose last increment also
+// computes the unit's scores), which therefore makes all of them visible
+// (release is cumulative).  On the consumer side lane 0 of each warp spins
+// with ld.acquire.gpu and __syncwarp() extends the acquire to its warp, whose
+// threads read the maps with L1::no_allocate loads (L2, never a stale L1
+// line from an earlier occupant of the slot).  Each item costs two CTA
+// barriers: step 1 -> step 2 of the FFT, and the end-of-item barrier.
 #pragma once
 
 #include "fastfft.cuh"
@@ -62,20 +66,19 @@ __device__ __forceinline__ int ld_acquire_gpu(const int* p) {
     return v;
 }
 
-// Thread 0 waits until *p >= target; bounded (about a second or more), then
-// flags the error and gives up.  A CTA barrier must follow before other
-// threads rely on the condition.
-__device__ __forceinline__ void wait_counter(const int* p, int target, int* error) {
-    if (threadIdx.x != 0) return;
-    if (ld_acquire_gpu(p) >= target) return;
-    for (int it = 0; it < (1 << 22); ++it) {
-        __nanosleep(256);
-        if (ld_acquire_gpu(p) >= target) {
-            __threadfence();
-            return;
+// The calling warp waits until *p >= target: lane 0 spins (bounded, about a
+// second or more, then flags the error and gives up) and __syncwarp()
+// extends its acquire to the warp.  Every lane must call it.
+__device__ __forceinline__ void wait_counter_warp(const int* p, int target, int* error) {
+    if ((threadIdx.x & 31) == 0 && ld_acquire_gpu(p) < target) {
+        bool ok = false;
+        for (int it = 0; it < (1 << 22) && !ok; ++it) {
+            __nanosleep(256);
+            ok = ld_acquire_gpu(p) >= target;
         }
+        if (!ok) atomicExch(error, 1);
     }
-    atomicExch(error, 1);
+    __syncwarp();
 }
 
 // b^-1 mod m for gcd(b, m) = 1 (compile time, m small)
@@ -87,8 +90,7 @@ constexpr int inv_mod(int b, int m) {
 
 // Tile geometry: V vectors per tile (16 or 8), 16 V threads per CTA (step 2
 // has one (vector, k1) task per thread), 512 / (16 V) CTAs per SM.  A pass of
-// one unit is T = L / V tiles and kDone = (warps per CTA) x T per-warp
-// completions, the same count (8 N2 x 45 / N2 ...) for both widths.
+// one unit is T = L / V tiles.
 template <int N2, int V_>
 struct CorrCfg {
     static constexpr int L = 16 * N2;
@@ -98,7 +100,7 @@ struct CorrCfg {
     static constexpr int kThreads = 16 * V;
     static constexpr int kWarps = kThreads / 32;
     static constexpr int T = L / V;
-    static constexpr int kDone = kWarps * T;
+    static constexpr int kDone = T;  // completions that finish one pass of a unit
     static constexpr int kCtasPerSm = 512 / kThreads;
     static_assert(V == 8 || V == 16, "tile width");
     // Odd N2 (l = 720 = 16 x 45): 16 and N2 are coprime, so both passes use
@@ -208,12 +210,6 @@ __device__ __forceinline__ void corr_row_tile(const CorrArgs& a, int u, int t, f
             st_l2hint(dst + 16 * k2, b[rf::rpos<N2>(k2)], keep);
         });
     }
-    // publish this warp's share of the tile
-    // (release: the warp's map stores, ordered by __syncwarp, become visible
-    // before the count; cheaper than a full fence + atomic)
-    __syncwarp();
-    if ((threadIdx.x & 31) == 0)
-        asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(&a.done_rows[u]) : "memory");
 }
 
 // Border mask of the map rows one column-pass thread produces: bit k2 is set
@@ -236,7 +232,7 @@ __device__ __forceinline__ uint2 corr_row_mask(int yb0, int yb1) {
 
 template <int N2, int V>
 __device__ __forceinline__ void corr_col_tile(const CorrArgs& a, int u, int t, float2* tile, const float2* twt,
-                                              uint2 ymask, bool* last_out) {
+                                              uint2 ymask) {
     using F = CorrCfg<N2, V>;
     constexpr int L = F::L;
     constexpr int h = L / 2;
@@ -318,19 +314,14 @@ __device__ __forceinline__ void corr_col_tile(const CorrArgs& a, int u, int t, f
     const double d2a = warp_sum((double)s2a), d2b = warp_sum((double)s2b);
     ka = warp_max_u64(ka);
     kb = warp_max_u64(kb);
-    // one set of atomics per warp (no CTA barrier)
-    bool last = false;
+    // one set of atomics per warp (published with the tile)
     if ((threadIdx.x & 31) == 0) {
         UnitAcc* ac = a.acc + 2 * (long long)u;
         if (ka) atomicMax(&ac[0].key, ka);
         atomicAdd(&ac[0].s2, d2a);
         if (kb) atomicMax(&ac[1].key, kb);
         atomicAdd(&ac[1].s2, d2b);
-        int prev;
-        asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;" : "=r"(prev) : "l"(&a.done_cols[u]) : "memory");
-        last = prev == F::kDone - 1;
     }
-    *last_out = last;  // meaningful in lane 0 only
 }
 
 // Score of one template from its accumulators (main.cu:869-876); s1 is the
@@ -350,17 +341,51 @@ __device__ __forceinline__ UnitOut unit_score(const UnitAcc& ac, double s1, int 
 }
 __device__ __forceinline__ UnitOut unit_score(const UnitAcc& ac, int l) { return unit_score(ac, ac.s1, l); }
 
-// Thread 0 claims and resolves the dependency of the next item while the
-// CTA works on the current one; one barrier publishes it.
+// Each warp checks the dependency of `item` before working on it.
 template <int N2, int V>
 __device__ __forceinline__ void corr_wait_for(const CorrArgs& a, int item) {
     using C = CorrCfg<N2, V>;
     const int s = item / (2 * C::T), j = item - s * (2 * C::T);
     if (j < C::T) {
-        if (s < a.nu && s >= a.S) wait_counter(a.done_cols + (s - a.S), C::kDone, a.error);
+        if (s < a.nu && s >= a.S) wait_counter_warp(a.done_cols + (s - a.S), C::kDone, a.error);
     } else {
         const int u = s - a.lag;
-        if (u >= 0 && u < a.nu) wait_counter(a.done_rows + u, C::kDone, a.error);
+        if (u >= 0 && u < a.nu) wait_counter_warp(a.done_rows + u, C::kDone, a.error);
+    }
+}
+
+// The publisher's part after the end-of-item barrier: count the finished
+// tile; the last column tile of a unit computes its two scores.
+template <int N2, int V>
+__device__ __forceinline__ void corr_publish(const CorrArgs& a, int item) {
+    using F = CorrCfg<N2, V>;
+    const int s = item / (2 * F::T), j = item - s * (2 * F::T);
+    if (j < F::T) {
+        if (s < a.nu) asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(&a.done_rows[s]) : "memory");
+        return;
+    }
+    const int u = s - a.lag;
+    if (u < 0 || u >= a.nu) return;
+    int prev;
+    asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;" : "=r"(prev) : "l"(&a.done_cols[u]) : "memory");
+    if (prev != F::kDone - 1) return;
+    const int2 wp = a.unit_wp[u];
+    const UnitAcc* ac = a.acc + 2 * (long long)u;
+    // sum of the map c1 + i c2 = L^2 S(0, 0), S = W conj(P)
+    // (frequency (0, 0) sits at element 0 in either column order)
+    const float2 w0 = __ldg(a.W + (long long)wp.x * a.L2);
+    const float2 p0 = __ldg(a.P + (long long)wp.y * a.L2);
+    const double sg = ((F::L / 2) % 2 == 0) ? 1.0 : -1.0;
+    const double l2 = (double)a.L2;
+    const double sums[2] = {sg * l2 * ((double)w0.x * p0.x + (double)w0.y * p0.y),
+                            sg * l2 * ((double)w0.y * p0.x - (double)w0.x * p0.y)};
+    for (int q = 0; q < 2; ++q) {
+        const int J = 2 * wp.y + q;
+        if (J >= a.ntmpl) break;
+        UnitAcc v;
+        v.key = __ldcg(&ac[q].key);
+        v.s2 = __ldcg(&ac[q].s2);
+        a.out[(long long)wp.x * a.ntmpl + J] = unit_score(v, sums[q], F::L);
     }
 }
 
@@ -368,10 +393,11 @@ template <int N2, int V>
 __global__ void __launch_bounds__(CorrCfg<N2, V>::kThreads, CorrCfg<N2, V>::kCtasPerSm) k_corr_persistent(CorrArgs a) {
     using F = CorrCfg<N2, V>;
     using SM = CorrSmem<N2, V>;
+    constexpr int kPub = F::kThreads - 1;  // the publisher
     extern __shared__ __align__(16) unsigned char smc[];
     float2* tile = reinterpret_cast<float2*>(smc);
     float2* twt = reinterpret_cast<float2*>(smc + SM::tile);
-    int* ish = reinterpret_cast<int*>(smc + SM::tile + SM::tw + SM::red);  // ring of 4 broadcast slots
+    int* ish = reinterpret_cast<int*>(smc + SM::tile + SM::tw + SM::red);  // ring of 4 claimed items
     // inverse twiddles W_L^{-n2 k1} = exp(+2 pi i n2 k1 / L), table [k1][n2]
     for (int i = threadIdx.x; i < (F::kPfa ? 0 : 16 * N2); i += F::kThreads) {
         const int k1 = i / N2, n2 = i - k1 * N2;
@@ -381,58 +407,33 @@ __global__ void __launch_bounds__(CorrCfg<N2, V>::kThreads, CorrCfg<N2, V>::kCta
     }
     const uint2 ymask = corr_row_mask<N2, V>(a.yb0, a.yb1);
     const int total = (a.nu + a.lag) * 2 * F::T;
-    if (threadIdx.x == 0) {
-        const int first = atomicAdd(a.next_item, 1);
-        if (first < total) corr_wait_for<N2, V>(a, first);
-        ish[0] = first;
+    // the CTA always holds its current item and the next one
+    if (threadIdx.x == kPub) {
+        ish[0] = atomicAdd(a.next_item, 1);
+        ish[1] = atomicAdd(a.next_item, 1);
     }
     __syncthreads();
     int item = ish[0];
-    for (int iter = 1; item < total; ++iter) {
-        int nxt = 0;
-        if (threadIdx.x == 0) nxt = atomicAdd(a.next_item, 1);  // consumed after the tile
+    for (int iter = 0; item < total; ++iter) {
+        corr_wait_for<N2, V>(a, item);
         const int s = item / (2 * F::T), j = item - s * (2 * F::T);
         if (j < F::T) {
-            if (s < a.nu) {
-                corr_row_tile<N2, V>(a, s, j, tile, twt);
-            }
+            if (s < a.nu) corr_row_tile<N2, V>(a, s, j, tile, twt);
         } else {
             const int u = s - a.lag;
-            if (u >= 0 && u < a.nu) {
-                bool last = false;
-                corr_col_tile<N2, V>(a, u, j - F::T, tile, twt, ymask, &last);
-                if ((threadIdx.x & 31) == 0 && last) {
-                    __threadfence();
-                    const int2 wp = a.unit_wp[u];
-                    const UnitAcc* ac = a.acc + 2 * (long long)u;
-                    // sum of the map c1 + i c2 = L^2 S(0, 0), S = W conj(P)
-                    // (frequency (0, 0) sits at element 0 in either column order)
-                    const float2 w0 = __ldg(a.W + (long long)wp.x * a.L2);
-                    const float2 p0 = __ldg(a.P + (long long)wp.y * a.L2);
-                    const double sg = ((F::L / 2) % 2 == 0) ? 1.0 : -1.0;
-                    const double l2 = (double)a.L2;
-                    const double sums[2] = {sg * l2 * ((double)w0.x * p0.x + (double)w0.y * p0.y),
-                                            sg * l2 * ((double)w0.y * p0.x - (double)w0.x * p0.y)};
-                    for (int q = 0; q < 2; ++q) {
-                        const int J = 2 * wp.y + q;
-                        if (J >= a.ntmpl) break;
-                        UnitAcc v;
-                        v.key = __ldcg(&ac[q].key);
-                        v.s2 = __ldcg(&ac[q].s2);
-                        a.out[(long long)wp.x * a.ntmpl + J] = unit_score(v, sums[q], F::L);
-                    }
-                }
-            }
+            if (u >= 0 && u < a.nu) corr_col_tile<N2, V>(a, u, j - F::T, tile, twt, ymask);
         }
-        if (threadIdx.x == 0) {
-            if (nxt < total) corr_wait_for<N2, V>(a, nxt);
-            ish[iter & 3] = nxt;
-        }
-        // one barrier: the tile buffer is free again and the next item (with its
-        // dependency satisfied) is published; slot iter & 3 is not rewritten
-        // before every thread has passed at least one more barrier
+        // every thread is done with the item: the tile buffer is free, the
+        // item's stores and atomics are ordered before its publication, and
+        // slot (iter + 1) & 3 (written two barriers ago) holds the next item;
+        // slot (iter + 2) & 3 was last read two iterations ago
         __syncthreads();
-        item = ish[iter & 3];
+        const int next = ish[(iter + 1) & 3];
+        if (threadIdx.x == kPub) {
+            corr_publish<N2, V>(a, item);
+            ish[(iter + 2) & 3] = atomicAdd(a.next_item, 1);
+        }
+        item = next;
     }
 }
 

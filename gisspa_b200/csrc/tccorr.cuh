@@ -277,7 +277,7 @@ __device__ __forceinline__ bool tc_col_tile(const CorrArgs& a, int u, int t, con
     return ok;
 }
 
-// The pipeline leader waits until *p >= target (bounded like wait_counter).
+// The pipeline leader waits until *p >= target (bounded like wait_counter_warp).
 __device__ __forceinline__ void tc_wait_counter(const int* p, int target, int* error) {
     if (ld_acquire_gpu(p) >= target) return;
     for (int it = 0; it < (1 << 22); ++it) {
