@@ -234,7 +234,10 @@ DTYPES = {"fp32": "f32", "tc-bf16": "bf16 hi+lo split, f32 accumulate",
           "tc-fp16": "fp16 hi+lo split, f32 accumulate"}
 
 
-TRAFFIC_PER_PAIR_UNIT_L720 = (10500180992 + 60203776) / 8800.0
+# DRAM bytes (read + write) of one persistent-kernel launch at window 720 per
+# (window, pair) unit, from an ncu capture of 88 windows x 100 pairs
+# (profiles/k_corr_persistent_l720_100pairs.md), scaled by units in the bench
+TRAFFIC_PER_PAIR_UNIT_L720 = (10417967872 + 49073664) / 8800.0
 
 
 def tensor_core_comparison(ds, kw, local_rank, base_precision: str):
