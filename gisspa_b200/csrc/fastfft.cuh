@@ -15,6 +15,8 @@
 // from one table entry per thread by at most three complex products.
 #pragma once
 
+#include <type_traits>
+
 #include "fft.cuh"
 #include "kernels.cuh"
 #include "regfft.cuh"
@@ -48,6 +50,14 @@ __device__ __forceinline__ void twiddle16(float2 w1, float2 (&w)[16]) {
 #pragma unroll
     for (int k = 9; k < 16; ++k) w[k] = cmul(w[8], w[k - 8]);
 }
+
+// IO functors with `static constexpr bool kStaged = true` store a row
+// transform's outputs in their own column order (column(k) for output k)
+// through shared memory (store_at(img, v, column, value)).
+template <class T, class = void>
+struct IoStaged : std::false_type {};
+template <class T>
+struct IoStaged<T, std::void_t<decltype(T::kStaged)>> : std::bool_constant<T::kStaged> {};
 
 template <int N2, bool kInv, bool kCols, class IO>
 __global__ void __launch_bounds__(256, 2) k_fft16(const float2* __restrict__ tw, IO io_param) {
@@ -85,10 +95,27 @@ __global__ void __launch_bounds__(256, 2) k_fft16(const float2* __restrict__ tw,
 #pragma unroll
         for (int n2 = 0; n2 < N2; ++n2) b[n2] = src[n2];
         rf::rfft<N2, 1, kInv>(b);
-        rf::static_for<N2>([&](auto kc) {
-            constexpr int k2 = decltype(kc)::value;
-            io.store(img, v0 + v, k1 + 16 * k2, b[rf::rpos<N2>(k2)]);
-        });
+        if constexpr (IoStaged<IO>::value) {
+            // permuted output order: through shared memory, so that the
+            // global stores stay coalesced
+            __syncthreads();  // every step-2 read of the tile is done
+            rf::static_for<N2>([&](auto kc) {
+                constexpr int k2 = decltype(kc)::value;
+                sm16[v * F::VP + io.column(k1 + 16 * k2)] = b[rf::rpos<N2>(k2)];
+            });
+        } else {
+            rf::static_for<N2>([&](auto kc) {
+                constexpr int k2 = decltype(kc)::value;
+                io.store(img, v0 + v, k1 + 16 * k2, b[rf::rpos<N2>(k2)]);
+            });
+        }
+    }
+    if constexpr (IoStaged<IO>::value) {
+        __syncthreads();
+        for (int e = threadIdx.x; e < F::V * F::L; e += F::kThreads) {
+            const int vv = e / F::L, p = e - vv * F::L;
+            io.store_at(img, v0 + vv, p, sm16[vv * F::VP + p]);
+        }
     }
     io.finish(reinterpret_cast<double*>(sm16 + F::V * F::VP));
 }
@@ -197,16 +224,22 @@ struct F16PairNorm {
     const float4* coef;
     int L;
     long long L2;
-    PfaCols pfa;  // pfa.N2 != 0: store the row spectra in prime-factor column order
     __device__ float2 load(int img, int v, int k) const {
         const float4 c = coef[img];
         const float2 z = data[f16_addr<false>(L, L2, img, v, k)];
         return make_float2((z.x - c.x) * c.y, -(z.y - c.z) * c.w);
     }
-    __device__ void store(int img, int v, int k, float2 x) const {
-        data[f16_addr<false>(L, L2, img, v, pfa.N2 ? pfa.physical(k) : k)] = x;
-    }
+    __device__ void store(int img, int v, int k, float2 x) const { data[f16_addr<false>(L, L2, img, v, k)] = x; }
     __device__ void finish(double*) const {}
+};
+
+// The same row pass, its spectra stored in the PfaCols column order of the
+// prime-factor correlation kernel.
+struct F16PairNormPfa : F16PairNorm {
+    PfaCols pfa;
+    static constexpr bool kStaged = true;
+    __device__ int column(int k) const { return pfa.physical(k); }
+    __device__ void store_at(int img, int v, int p, float2 x) const { data[f16_addr<false>(L, L2, img, v, p)] = x; }
 };
 
 // Row pass of the correlation: S = W_w conj(P_p), inverse FFT along x,

@@ -386,7 +386,11 @@ static int pair_spectra(gs_ctx* ctx, float e, float2* TS, bool pfa = false) {
     ++ctx->counters.kernel_launches;
     CKL();
     if (fast_ok(ctx, l)) {
-        TRY(run_fast<false, false>(ctx, l, Np, F16PairNorm{TS, P<float4>(ctx->coef), l, l2, pfa ? PfaCols::make(l) : PfaCols{}}));
+        const F16PairNorm rows{TS, P<float4>(ctx->coef), l, l2};
+        if (pfa)
+            TRY(run_fast<false, false>(ctx, l, Np, F16PairNormPfa{rows, PfaCols::make(l)}));
+        else
+            TRY(run_fast<false, false>(ctx, l, Np, rows));
         TRY(run_fast<false, true>(ctx, l, Np, F16Complex<true>{TS, l, l2, (float)(1.0 / (double)l2)}));
     } else {
         TRY(run_fft<false>(ctx, l, rows_of(l, l), Np, IoPairNorm{TS, P<float4>(ctx->coef), l2}));

@@ -430,11 +430,17 @@ __global__ void __launch_bounds__(256) k_pair_rotate(const float* __restrict__ t
     const int npix = l * l;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < npix; q += gridDim.x * blockDim.x) {
         const int i = q % l, j = q / l;
+        // mask first: outside radius rout the product with the mask is 0
+        // whatever the rotated value, so its gathers are skipped
+        const float r = hypotf((float)(i - h), (float)(j - h));
+        float m = 1.0f;
+        if (r > rout) m = 0.0f;
+        else if (r >= rin) m = (float)(0.5 * (double)cosf((float)(kPiRef * (double)(r - rin) / 12.0)) + 0.5);
         const float x = (float)(i - h), y = (float)(j - h);
         const float x2 = (cose * x + sine * y) + h;
         const float y2 = (-sine * x + cose * y) + h;
         float v1 = 0.0f, v2 = 0.0f;
-        if (!(x2 < 0 || x2 > l - 1.0f || y2 < 0 || y2 > l - 1.0f)) {
+        if (m != 0.0f && !(x2 < 0 || x2 > l - 1.0f || y2 < 0 || y2 > l - 1.0f)) {
             const int ii = (int)floorf(x2), jj = (int)floorf(y2);
             const int k0 = ii + jj * l;
             int k1 = k0 + 1, k2 = k0 + l + 1, k3 = k0 + l;
@@ -446,10 +452,6 @@ __global__ void __launch_bounds__(256) k_pair_rotate(const float* __restrict__ t
             if (has2)
                 v2 = __ldg(t2 + k0) * tt * uu + __ldg(t2 + k1) * t * uu + __ldg(t2 + k2) * t * u + __ldg(t2 + k3) * tt * u;
         }
-        const float r = hypotf((float)(i - h), (float)(j - h));
-        float m = 1.0f;
-        if (r > rout) m = 0.0f;
-        else if (r >= rin) m = (float)(0.5 * (double)cosf((float)(kPiRef * (double)(r - rin) / 12.0)) + 0.5);
         v1 *= m;
         v2 *= m;
         o[q] = make_float2(v1, v2);
