@@ -36,8 +36,10 @@
 // (release is cumulative).  On the consumer side lane 0 of each warp spins
 // with ld.acquire.gpu and __syncwarp() extends the acquire to its warp, whose
 // threads read the maps with L1::no_allocate loads (L2, never a stale L1
-// line from an earlier occupant of the slot).  Each item costs two CTA
-// barriers: step 1 -> step 2 of the FFT, and the end-of-item barrier.
+// line from an earlier occupant of the slot).  A column tile costs two CTA
+// barriers (step 1 -> step 2 of the FFT, whose vectors are columns spread
+// over all warps for coalesced loads, and the end-of-item barrier); a row
+// tile only the end-of-item barrier, as each warp owns two whole rows.
 #pragma once
 
 #include "fastfft.cuh"
@@ -103,6 +105,7 @@ struct CorrCfg {
     static constexpr int kDone = T;  // completions that finish one pass of a unit
     static constexpr int kCtasPerSm = 512 / kThreads;
     static_assert(V == 8 || V == 16, "tile width");
+    static_assert(V == 2 * kWarps, "a row tile gives each warp two rows");
     // Odd N2 (l = 720 = 16 x 45): 16 and N2 are coprime, so both passes use
     // the Good-Thomas mapping and need no twiddles between their two DFT
     // steps.  Along x the spectra arrive in that mapping's input order
@@ -180,8 +183,11 @@ __device__ __forceinline__ void corr_row_tile(const CorrArgs& a, int u, int t, f
     float2* Rs = a.R + (long long)(u % a.S) * a.L2;
     const int r0 = t * F::V;
     const unsigned long long keep = l2_policy_evict_last();
-    for (int task = threadIdx.x; task < F::V * N2; task += F::kThreads) {
-        const int v = task / N2, n2 = task - v * N2;
+    // each warp transforms its own two rows (vectors 2w, 2w + 1) through its
+    // own part of the tile buffer, so step 1 -> step 2 needs only __syncwarp
+    const int w2 = 2 * (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    for (int task = lane; task < 2 * N2; task += 32) {
+        const int v = w2 + (task >= N2), n2 = task - (task >= N2) * N2;
         const long long base = (long long)F::spectrum_row(r0 + v) * L + n2;
         float2 x[16];
 #pragma unroll
@@ -196,9 +202,9 @@ __device__ __forceinline__ void corr_row_tile(const CorrArgs& a, int u, int t, f
             dst[k1 * F::BP] = (k1 && !F::kPfa) ? cmul(x[r], tw[k1 * N2]) : x[r];
         });
     }
-    __syncthreads();
+    __syncwarp();
     {
-        const int v = threadIdx.x >> 4, k1 = threadIdx.x & 15;
+        const int v = threadIdx.x >> 4, k1 = threadIdx.x & 15;  // v = w2 + lane / 16
         float2 b[N2];
         const float2* src = tile + v * F::VP + k1 * F::BP;
 #pragma unroll
