@@ -118,7 +118,7 @@ struct CorrCfg {
     static constexpr int A1 = kPfa ? (N2 * inv_mod(N2 % 16, 16)) % L : 1;
     static constexpr int A2 = kPfa ? (16 * inv_mod(16 % N2, N2)) % L : 16;
     // spectrum row that physical row r of the scratch map holds
-    __device__ __forceinline__ static int spectrum_row(int r) {
+    __host__ __device__ __forceinline__ static int spectrum_row(int r) {
         if constexpr (kPfa) {
             const int n1 = r / N2, n2 = r - n1 * N2;
             const int q = N2 * n1 + 16 * n2;
