@@ -16,11 +16,14 @@
 // Dependencies and why they cannot deadlock: a column tile of u waits until
 // all T row tiles of u are done; a row tile of u >= S waits until all
 // column tiles of u - S are done (its scratch slot is free).  Completion is
-// counted per tile: after the CTA barrier that ends a tile, one thread (the
-// publisher, the CTA's last thread, which has the lightest share of step 1
-// when the tasks do not divide evenly) increments the unit's counter, so a
-// pass of a unit is done at T increments.  Each warp checks the dependency of
-// its CTA's next item itself before starting it.  Both dependencies point at
+// counted per tile or per warp (CorrCfg::kWarpPub).  Per tile: after the CTA
+// barrier that ends a tile, one thread (the publisher, the CTA's last thread,
+// which has the lightest share of step 1 when the tasks do not divide evenly)
+// increments the unit's counter, so a pass of a unit is done at T
+// increments, and each warp checks the dependency of its CTA's next item
+// itself before starting it.  Per warp: every warp counts its own share
+// before that barrier (a pass is done at warps x T increments), and thread 0
+// waits for the next item's dependency before it.  Both dependencies point at
 // items that come earlier in the claim order, and an item is claimed only by
 // a running CTA that finishes and publishes it before it waits for anything
 // later, so the earliest unpublished item can always proceed.  Every wait is
@@ -30,12 +33,12 @@
 //
 // Memory ordering: producers store the maps bypassing L1 (st.global with an
 // L2 cache hint) and add their accumulator atomics; the CTA barrier that ends
-// the tile orders every thread's stores before the publisher's release
-// increment (acquire-release for column tiles, whose last increment also
+// the tile (per warp: __syncwarp) orders every thread's stores before the
+// release increment (acquire-release for column tiles, whose last increment also
 // computes the unit's scores), which therefore makes all of them visible
-// (release is cumulative).  On the consumer side lane 0 of each warp spins
-// with ld.acquire.gpu and __syncwarp() extends the acquire to its warp, whose
-// threads read the maps with L1::no_allocate loads (L2, never a stale L1
+// (release is cumulative).  On the consumer side lane 0 of each warp (per
+// warp: thread 0) spins with ld.acquire.gpu and __syncwarp() (the barrier)
+// extends the acquire to its warp (CTA), whose threads read the maps with L1::no_allocate loads (L2, never a stale L1
 // line from an earlier occupant of the slot).  A column tile costs two CTA
 // barriers (step 1 -> step 2 of the FFT, whose vectors are columns spread
 // over all warps for coalesced loads, and the end-of-item barrier); a row
@@ -68,18 +71,24 @@ __device__ __forceinline__ int ld_acquire_gpu(const int* p) {
     return v;
 }
 
+// The calling thread waits until *p >= target (bounded: about a second or
+// more, then it flags the error and gives up).  A barrier must follow before
+// other threads rely on the condition.
+__device__ __forceinline__ void wait_counter(const int* p, int target, int* error) {
+    if (ld_acquire_gpu(p) >= target) return;
+    bool ok = false;
+    for (int it = 0; it < (1 << 22) && !ok; ++it) {
+        __nanosleep(256);
+        ok = ld_acquire_gpu(p) >= target;
+    }
+    if (!ok) atomicExch(error, 1);
+}
+
 // The calling warp waits until *p >= target: lane 0 spins (bounded, about a
 // second or more, then flags the error and gives up) and __syncwarp()
 // extends its acquire to the warp.  Every lane must call it.
 __device__ __forceinline__ void wait_counter_warp(const int* p, int target, int* error) {
-    if ((threadIdx.x & 31) == 0 && ld_acquire_gpu(p) < target) {
-        bool ok = false;
-        for (int it = 0; it < (1 << 22) && !ok; ++it) {
-            __nanosleep(256);
-            ok = ld_acquire_gpu(p) >= target;
-        }
-        if (!ok) atomicExch(error, 1);
-    }
+    if ((threadIdx.x & 31) == 0) wait_counter(p, target, error);
     __syncwarp();
 }
 
@@ -102,7 +111,16 @@ struct CorrCfg {
     static constexpr int kThreads = 16 * V;
     static constexpr int kWarps = kThreads / 32;
     static constexpr int T = L / V;
-    static constexpr int kDone = T;  // completions that finish one pass of a unit
+    // Publication protocol.  When step 1's tasks do not divide evenly over
+    // the threads (odd N2), per tile: one thread publishes after the
+    // end-of-item barrier -- the CTA's last thread, whose step-1 share is the
+    // lightest, so the release fence it waits for costs no barrier time --
+    // and every warp checks its next item's dependency itself.  Otherwise
+    // (kWarpPub) per warp: lane 0 of every warp counts its own share before
+    // that barrier, and thread 0 waits for the next item's dependency while
+    // the CTA finishes the current one.  Each was measured faster where used.
+    static constexpr bool kWarpPub = (V * N2) % (16 * V) == 0;
+    static constexpr int kDone = kWarpPub ? (V / 2) * T : T;  // completions that finish one pass of a unit
     static constexpr int kCtasPerSm = 512 / kThreads;
     static_assert(V == 8 || V == 16, "tile width");
     static_assert(V == 2 * kWarps, "a row tile gives each warp two rows");
@@ -347,21 +365,27 @@ __device__ __forceinline__ UnitOut unit_score(const UnitAcc& ac, double s1, int 
 }
 __device__ __forceinline__ UnitOut unit_score(const UnitAcc& ac, int l) { return unit_score(ac, ac.s1, l); }
 
-// Each warp checks the dependency of `item` before working on it.
+// The counter whose completions `item` waits for (kDone of them), or nullptr.
+template <int N2, int V>
+__device__ __forceinline__ const int* corr_dep(const CorrArgs& a, int item) {
+    using C = CorrCfg<N2, V>;
+    const int s = item / (2 * C::T), j = item - s * (2 * C::T);
+    if (j < C::T) return (s < a.nu && s >= a.S) ? a.done_cols + (s - a.S) : nullptr;
+    const int u = s - a.lag;
+    return (u >= 0 && u < a.nu) ? a.done_rows + u : nullptr;
+}
+
+// Per-tile protocol: each warp checks the dependency of `item` before
+// working on it.
 template <int N2, int V>
 __device__ __forceinline__ void corr_wait_for(const CorrArgs& a, int item) {
     using C = CorrCfg<N2, V>;
-    const int s = item / (2 * C::T), j = item - s * (2 * C::T);
-    if (j < C::T) {
-        if (s < a.nu && s >= a.S) wait_counter_warp(a.done_cols + (s - a.S), C::kDone, a.error);
-    } else {
-        const int u = s - a.lag;
-        if (u >= 0 && u < a.nu) wait_counter_warp(a.done_rows + u, C::kDone, a.error);
-    }
+    const int* p = corr_dep<N2, V>(a, item);
+    if (p) wait_counter_warp(p, C::kDone, a.error);
 }
 
-// The publisher's part after the end-of-item barrier: count the finished
-// tile; the last column tile of a unit computes its two scores.
+// Count a finished tile (or one warp's share of it, kWarpPub); the last
+// count of a unit's column pass computes its two scores.
 template <int N2, int V>
 __device__ __forceinline__ void corr_publish(const CorrArgs& a, int item) {
     using F = CorrCfg<N2, V>;
@@ -413,7 +437,45 @@ __global__ void __launch_bounds__(CorrCfg<N2, V>::kThreads, CorrCfg<N2, V>::kCta
     }
     const uint2 ymask = corr_row_mask<N2, V>(a.yb0, a.yb1);
     const int total = (a.nu + a.lag) * 2 * F::T;
-    // the CTA always holds its current item and the next one
+    if constexpr (F::kWarpPub) {
+        // per-warp protocol: thread 0 claims the next item while the CTA works
+        // on the current one and resolves its dependency before the barrier
+        // that ends the current one (each warp has counted its share by then,
+        // thread 0's own warp included, so nothing of this CTA is pending)
+        if (threadIdx.x == 0) {
+            const int first = atomicAdd(a.next_item, 1);
+            const int* p = first < total ? corr_dep<N2, V>(a, first) : nullptr;
+            if (p) wait_counter(p, F::kDone, a.error);
+            ish[0] = first;
+        }
+        __syncthreads();
+        int item = ish[0];
+        for (int iter = 1; item < total; ++iter) {
+            int nxt = 0;
+            if (threadIdx.x == 0) nxt = atomicAdd(a.next_item, 1);  // consumed after the tile
+            const int s = item / (2 * F::T), j = item - s * (2 * F::T);
+            if (j < F::T) {
+                if (s < a.nu) corr_row_tile<N2, V>(a, s, j, tile, twt);
+            } else {
+                const int u = s - a.lag;
+                if (u >= 0 && u < a.nu) corr_col_tile<N2, V>(a, u, j - F::T, tile, twt, ymask);
+            }
+            __syncwarp();  // the warp's stores and atomics before its count
+            if ((threadIdx.x & 31) == 0) corr_publish<N2, V>(a, item);
+            if (threadIdx.x == 0) {
+                const int* p = nxt < total ? corr_dep<N2, V>(a, nxt) : nullptr;
+                if (p) wait_counter(p, F::kDone, a.error);
+                ish[iter & 3] = nxt;
+            }
+            // the tile buffer is free and the next item (dependency satisfied)
+            // published; slot iter & 3 is not rewritten before every thread has
+            // passed at least one more barrier
+            __syncthreads();
+            item = ish[iter & 3];
+        }
+        return;
+    }
+    // per-tile protocol: the CTA always holds its current item and the next one
     if (threadIdx.x == kPub) {
         ish[0] = atomicAdd(a.next_item, 1);
         ish[1] = atomicAdd(a.next_item, 1);
