@@ -237,7 +237,7 @@ DTYPES = {"fp32": "f32", "tc-bf16": "bf16 hi+lo split, f32 accumulate",
 # DRAM bytes (read + write) of one persistent-kernel launch at window 720 per
 # (window, pair) unit, from an ncu capture of 88 windows x 100 pairs
 # (profiles/k_corr_persistent_l720_100pairs.md), scaled by units in the bench
-TRAFFIC_PER_PAIR_UNIT_L720 = (10417967872 + 49073664) / 8800.0
+TRAFFIC_PER_PAIR_UNIT_L720 = (10585217280 + 106544128) / 8800.0
 
 
 def tensor_core_comparison(ds, kw, local_rank, base_precision: str):
