@@ -24,6 +24,7 @@ LIB_PATH = os.path.join(HERE, "lib", "libgisspa_b200.so")
 DRIVER_PATH = os.path.join(HERE, "lib", "gisspa_main")
 
 GS_OK = 0
+GS_ERR_ARG, GS_ERR_OOM, GS_ERR_CUDA, GS_ERR_STATE, GS_ERR_UNSUPPORTED, GS_ERR_TIMEOUT, GS_ERR_IO = range(1, 8)
 STATUS = {0: "ok", 1: "invalid argument", 2: "out of memory", 3: "CUDA error",
           4: "invalid call order", 5: "unsupported input", 6: "device wait timed out",
           7: "I/O error"}
@@ -76,7 +77,8 @@ EXPORTS = ("gs_status_string", "gs_version", "gs_params_default", "gs_ctx_create
            "gs_search", "gs_search_device", "gs_get_units", "gs_picks_free", "gs_get_timings",
            "gs_get_stats", "gs_set_kernel_timing", "gs_set_option",
            "gs_correlate_window_noalloc", "gs_search_batch", "gs_get_tuning", "gs_score_grad",
-           "gs_refine", "gs_merge_duplicates")
+           "gs_refine", "gs_merge_duplicates", "gs_hdf_read_image", "gs_hdf_read_dataset",
+           "gs_hdf_read_attribute", "gs_host_free")
 
 _lib_handle = None
 
@@ -130,9 +132,99 @@ def load_library(path: Optional[str] = None) -> C.CDLL:
     lib.gs_refine.argtypes = [vp, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
     lib.gs_merge_duplicates.argtypes = [C.c_int, C.c_void_p, C.c_size_t, C.c_double, C.c_double,
                                         C.c_void_p]
+    lib.gs_hdf_read_image.argtypes = [C.c_char_p, C.c_int, C.POINTER(C.POINTER(C.c_float)),
+                                      C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                      C.c_char_p, C.c_size_t]
+    lib.gs_hdf_read_dataset.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(C.POINTER(C.c_double)),
+                                        C.POINTER(C.c_int64), C.POINTER(C.c_int), C.c_char_p, C.c_size_t]
+    lib.gs_hdf_read_attribute.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.POINTER(C.c_double),
+                                          C.c_size_t, C.POINTER(C.c_size_t), C.c_char_p, C.c_size_t,
+                                          C.c_char_p, C.c_size_t]
+    lib.gs_host_free.argtypes = [C.c_void_p]
+    lib.gs_host_free.restype = None
     if path is None:
         _lib_handle = lib
     return lib
+
+
+_HDF5_SIGNATURE = b"\x89HDF\r\n\x1a\n"
+
+
+def is_hdf5(path: str) -> bool:
+    """The file starts with the HDF5 signature (EMhdf::is_valid,
+    EMReader/emhdf_.cpp:47-62)."""
+    try:
+        with open(path, "rb") as fh:
+            return fh.read(8) == _HDF5_SIGNATURE
+    except OSError:
+        return False
+
+
+def read_hdf_image(path: str, index: int = 0) -> np.ndarray:
+    """Image ``index`` of an EMAN HDF5 file (old EMAN or EMAN2 layout) as
+    float32, shape (ny, nx) or (nz, ny, nx), through gs_hdf_read_image."""
+    lib = load_library()
+    data = C.POINTER(C.c_float)()
+    nx, ny, nz = C.c_int(), C.c_int(), C.c_int()
+    err = C.create_string_buffer(512)
+    st = lib.gs_hdf_read_image(path.encode(), int(index), C.byref(data), C.byref(nx), C.byref(ny),
+                               C.byref(nz), err, len(err))
+    if st != GS_OK:
+        raise GisspaError(st, err.value.decode(errors="replace"))
+    try:
+        n = nx.value * ny.value * nz.value
+        a = np.ctypeslib.as_array(data, (n,)).copy()
+    finally:
+        lib.gs_host_free(data)
+    shape = (ny.value, nx.value) if nz.value == 1 else (nz.value, ny.value, nx.value)
+    return a.reshape(shape)
+
+
+def read_hdf_dataset(path: str, name: str) -> np.ndarray:
+    """Any numeric dataset of an HDF5 file as float64 (gs_hdf_read_dataset)."""
+    lib = load_library()
+    data = C.POINTER(C.c_double)()
+    dims = (C.c_int64 * 8)()
+    rank = C.c_int()
+    err = C.create_string_buffer(512)
+    st = lib.gs_hdf_read_dataset(path.encode(), name.encode(), C.byref(data), dims, C.byref(rank), err,
+                                 len(err))
+    if st != GS_OK:
+        raise GisspaError(st, err.value.decode(errors="replace"))
+    try:
+        shape = tuple(int(dims[k]) for k in range(rank.value))
+        n = int(np.prod(shape)) if shape else 1
+        a = np.ctypeslib.as_array(data, (n,)).copy() if n else np.zeros(0)
+    finally:
+        lib.gs_host_free(data)
+    return a.reshape(shape)
+
+
+def read_hdf_attribute(path: str, obj: str, name: str):
+    """Attribute ``name`` of HDF5 object ``obj``: a float64 array, or a str for
+    a fixed-length string (gs_hdf_read_attribute)."""
+    lib = load_library()
+    vals = (C.c_double * 64)()
+    nv = C.c_size_t()
+    text = C.create_string_buffer(1024)
+    err = C.create_string_buffer(512)
+    st = lib.gs_hdf_read_attribute(path.encode(), obj.encode(), name.encode(), vals, 64, C.byref(nv), text,
+                                   len(text), err, len(err))
+    if st != GS_OK:
+        raise GisspaError(st, err.value.decode(errors="replace"))
+    if nv.value == 0 and text.value:
+        return text.value.decode(errors="replace")
+    return np.array([vals[k] for k in range(min(nv.value, 64))])
+
+
+def read_image(path: str, section: int = -1) -> np.ndarray:
+    """emdata::readImage (EMReader/emdata_.cpp:174-205): image ``section`` of
+    an EMAN HDF5 file, else section ``section`` of an MRC file (the whole
+    stack for an out-of-range section)."""
+    from . import formats
+    if is_hdf5(path):
+        return read_hdf_image(path, section)
+    return formats.read_mrc(path, section)
 
 
 def default_params(**kw) -> GsParams:
@@ -424,11 +516,14 @@ def run_config(config_path: str, device: Optional[int] = None, return_units: boo
         raise ValueError("missing required keys: %s" % ", ".join(missing))
     eul = formats.read_euler(cfg.eulerf)
     n = eul.shape[0]
-    h = formats.read_mrc_header(cfg.temp2d)
-    whole = formats.read_mrc(cfg.temp2d, -1)
-    if whole.ndim == 2:
-        whole = whole[None]
-    stack = np.stack([whole[J] if J < whole.shape[0] else whole[0] for J in range(n)])
+    if is_hdf5(cfg.temp2d):
+        # one image per template (readAndPaddingTemplate, main.cu:186-190)
+        stack = np.stack([read_hdf_image(cfg.temp2d, J) for J in range(n)])
+    else:
+        whole = formats.read_mrc(cfg.temp2d, -1)
+        if whole.ndim == 2:
+            whole = whole[None]
+        stack = np.stack([whole[J] if J < whole.shape[0] else whole[0] for J in range(n)])
     first = formats.read_lst_entry(cfg.inlst, cfg.first)
     if first is None:
         raise IOError("entry %d of %s not found" % (cfg.first, cfg.inlst))
@@ -442,7 +537,7 @@ def run_config(config_path: str, device: Optional[int] = None, return_units: boo
             ent = formats.read_lst_entry(cfg.inlst, m)
             if ent is None:
                 raise IOError("entry %d of %s not found" % (m, cfg.inlst))
-            img = formats.read_mrc(ent.path, ent.nn)
+            img = read_image(ent.path, ent.nn)
             if img.ndim == 3:
                 img = img[0]
             picks = ctx.search(img, (ent.defocus, ent.dfdiff, ent.dfang))

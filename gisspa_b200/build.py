@@ -44,6 +44,7 @@ def _run(cmd, cwd=None) -> None:
 
 def build_library(force: bool = False) -> str:
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cuh"))
+                  + glob.glob(os.path.join(CSRC, "*.cpp"))
                   + [os.path.join(INCLUDE, "gisspa.h")])
     if not force and _newer(LIB, srcs):
         return LIB
@@ -51,7 +52,8 @@ def build_library(force: bool = False) -> str:
     _run([NVCC] + NVCC_FLAGS + ARCH + ["-shared", "-I" + INCLUDE, "-o", LIB,
                                        os.path.join(CSRC, "gisspa.cu"),
                                        os.path.join(CSRC, "noalloc.cu"),
-                                       os.path.join(CSRC, "merge.cu")])
+                                       os.path.join(CSRC, "merge.cu"),
+                                       os.path.join(CSRC, "hdf5io.cpp"), "-lz"])
     return LIB
 
 

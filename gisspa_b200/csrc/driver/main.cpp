@@ -111,9 +111,10 @@ int main(int argc, char** argv) {
     }
     const CtfState ctf_first = ctf;
 
-    // template stack: section J for template J (main.cu:182-223)
+    // template stack: section (MRC) or image (EMAN HDF5) J for template J
+    // (main.cu:182-223)
     Image t0;
-    std::string err = read_mrc(cfg.temp2d, 0, &t0);
+    std::string err = read_image(cfg.temp2d, 0, &t0);
     if (!err.empty()) {
         fprintf(stderr, "%s\n", err.c_str());
         fclose(fp);
@@ -121,7 +122,18 @@ int main(int argc, char** argv) {
     }
     const int tx = t0.nx, ty = t0.ny;
     std::vector<float> stack((size_t)ntmpl * tx * ty);
-    {
+    if (is_hdf5(cfg.temp2d)) {
+        for (int J = 0; J < ntmpl; ++J) {
+            Image tj;
+            err = read_image(cfg.temp2d, J, &tj);
+            if (!err.empty() || tj.nx != tx || tj.ny != ty || tj.nz != 1) {
+                fprintf(stderr, "%s\n", err.empty() ? "template images differ in size" : err.c_str());
+                fclose(fp);
+                return 1;
+            }
+            memcpy(stack.data() + (size_t)J * tx * ty, tj.data.data(), sizeof(float) * tx * ty);
+        }
+    } else {
         Image all;
         err = read_mrc(cfg.temp2d, -1, &all);
         if (!err.empty() || all.nx != tx || all.ny != ty) {
@@ -162,7 +174,7 @@ int main(int argc, char** argv) {
             return 1;
         }
         Image mic;
-        err = read_mrc(ent.path, ent.nn, &mic);
+        err = read_image(ent.path, ent.nn, &mic);
         if (!err.empty()) {
             fprintf(stderr, "%s\n", err.c_str());
             fclose(fp);

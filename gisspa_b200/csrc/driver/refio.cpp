@@ -1,5 +1,7 @@
 #include "refio.hpp"
 
+#include "gisspa.h"
+
 #include <cctype>
 #include <cstdint>
 #include <cstdio>
@@ -227,6 +229,31 @@ std::string read_mrc(const std::string& path, int section, Image* img) {
             img->data[i] = v;
         }
     }
+    return "";
+}
+
+bool is_hdf5(const std::string& path) {
+    static const unsigned char sig[8] = {0x89, 'H', 'D', 'F', '\r', '\n', 0x1a, '\n'};
+    FILE* f = fopen(path.c_str(), "rb");
+    if (!f) return false;
+    unsigned char s[8] = {0};
+    const bool ok = fread(s, 1, 8, f) == 8 && memcmp(s, sig, 8) == 0;
+    fclose(f);
+    return ok;
+}
+
+std::string read_image(const std::string& path, int section, Image* img) {
+    if (!is_hdf5(path)) return read_mrc(path, section, img);
+    float* data = nullptr;
+    int nx = 0, ny = 0, nz = 0;
+    char err[512];
+    const int st = gs_hdf_read_image(path.c_str(), section, &data, &nx, &ny, &nz, err, sizeof err);
+    if (st != GS_OK) return std::string(err[0] ? err : gs_status_string(st));
+    img->nx = nx;
+    img->ny = ny;
+    img->nz = nz;
+    img->data.assign(data, data + (size_t)nx * ny * nz);
+    gs_host_free(data);
     return "";
 }
 

@@ -4,6 +4,7 @@
 //  - Euler file    : DataReader.cpp:267-284 ("alt az" per line)
 //  - input list    : DataReader.cpp:318-388 (#LST / #LSX), main.cu:125-138 (path prefix)
 //  - MRC image     : EMReader/emdata_.cpp:384-617 (modes 0/1/2/4, byte order, sections)
+//  - EMAN HDF5     : EMReader/emdata_.cpp:174-199 dispatch, read by gs_hdf_read_image
 #pragma once
 
 #include <string>
@@ -55,5 +56,10 @@ struct Image {
 // Section `section` of an MRC file (whole volume if out of range).  Returns
 // an empty string on success, otherwise the reason.
 std::string read_mrc(const std::string& path, int section, Image* img);
+// The file starts with the HDF5 signature (EMhdf::is_valid, emhdf_.cpp:47-62).
+bool is_hdf5(const std::string& path);
+// emdata::readImage (emdata_.cpp:174-205): image `section` of an EMAN HDF5
+// file (gs_hdf_read_image), else section `section` of an MRC file.
+std::string read_image(const std::string& path, int section, Image* img);
 
 }  // namespace gsdrv

@@ -308,6 +308,40 @@ typedef struct gs_stats {
 } gs_stats;
 int gs_get_stats(struct gs_ctx* ctx, gs_stats* out);
 
+/* EMAN HDF5 input (host only; needs no GPU and no context).  Replaces the
+ * reference's HDF5 branch of emdata::readImage (EMReader/emdata_.cpp:174-199)
+ * with libhdf5 behind it: EMhdf (old style, EMReader/emhdf_.cpp:95-265,
+ * chosen when the root group has a num_dataset attribute; image `index` is the
+ * root dataset named by the index, nx / ny / nz = dims[0] / dims[1] / dims[2]
+ * of its dataspace, floating-point data only, equal spacing_row / spacing_col /
+ * spacing_sec required) and EMhdf2 (EMAN2 style, EMReader/emhdf2_.cpp:245-362:
+ * dataset /MDF/images/<index>/image sized by the EMAN.nx / EMAN.ny / EMAN.nz
+ * attributes of its group, integer or float data converted to float).  A
+ * negative index reads image 0.  The file must start with the HDF5 signature
+ * (EMhdf::is_valid).  On success *host_data holds nx * ny * nz floats, x
+ * fastest, to be released with gs_host_free.  Where the reference falls back
+ * to a 10 x 10 zero image (missing image, no size attributes, anisotropic
+ * spacing, size mismatch) this returns GS_ERR_IO with the reason in `err`;
+ * HDF5 features outside what the parser reads (dense link or attribute
+ * storage, variable-length or compound data, chunk indexes other than the
+ * version 1 B-tree and the single chunk, filters other than deflate / shuffle /
+ * Fletcher-32) return GS_ERR_UNSUPPORTED. */
+int gs_hdf_read_image(const char* path, int index, float** host_data, int* nx, int* ny, int* nz,
+                      char* err, size_t err_len);
+/* Any numeric dataset of an HDF5 file (user block allowed), converted to
+ * double, row-major; dims[0..*rank-1] receive its extents (rank <= 8; a
+ * scalar has rank 0 and one value).  Release with gs_host_free.  No reference
+ * counterpart: an inspection helper over the same parser. */
+int gs_hdf_read_dataset(const char* path, const char* dataset, double** host_data, int64_t* dims, int* rank,
+                        char* err, size_t err_len);
+/* Attribute `name` of the group or dataset `object`: numeric values (the
+ * first max_values, converted to double; *n_values = their count) or, for a
+ * fixed-length string, its text in `text`.  No reference counterpart. */
+int gs_hdf_read_attribute(const char* path, const char* object, const char* name, double* values,
+                          size_t max_values, size_t* n_values, char* text, size_t text_len, char* err,
+                          size_t err_len);
+void gs_host_free(void* p);
+
 /* Correlation of one window with a set of templates, allocating nothing.
  * This entry point has no counterpart in the reference; it serves callers
  * that may not allocate device memory while they run (code being captured
