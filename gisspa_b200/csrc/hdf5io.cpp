@@ -59,8 +59,8 @@ uint64_t le(const uint8_t* p, int n) {
 struct Cur {
     const std::vector<uint8_t>* b;
     size_t p;
-    const uint8_t* at(size_t n) const {
-        if (p + n > b->size()) fail_io("HDF5 structure runs past its block");
+    const uint8_t* at(uint64_t n) const {
+        if (p > b->size() || n > b->size() - p) fail_io("HDF5 structure runs past its block");
         return b->data() + p;
     }
     uint64_t u(int n) {
@@ -68,9 +68,9 @@ struct Cur {
         p += (size_t)n;
         return v;
     }
-    void skip(size_t n) {
+    void skip(uint64_t n) {
         at(n);
-        p += n;
+        p += (size_t)n;
     }
 };
 
@@ -90,10 +90,14 @@ struct DType {
 struct Space {
     bool null = false;
     std::vector<uint64_t> dims;  // empty: scalar
+    // number of elements, saturating at 2^62 (no wrap-around for corrupt dims)
     uint64_t count() const {
         if (null) return 0;
         uint64_t n = 1;
-        for (uint64_t d : dims) n *= d;
+        for (uint64_t d : dims) {
+            if (d == 0) return 0;
+            n = (n > (1ull << 62) / d) ? (1ull << 62) : n * d;
+        }
         return n;
     }
 };
@@ -342,7 +346,7 @@ class File {
     std::vector<uint8_t> raw(const Dataset& d) const {
         const uint64_t es = (uint64_t)d.t.size;
         const uint64_t n = d.s.count();
-        if (n > (1ull << 32) / std::max<uint64_t>(es, 1)) fail_unsupported("HDF5 dataset above 4 GB");
+        if (n > (1ull << 31) / std::max<uint64_t>(es, 1)) fail_unsupported("HDF5 dataset above 2 GB");
         const uint64_t bytes = n * es;
         if (d.lay.cls == 0) {
             if (d.lay.compact.size() < bytes) fail_io("short compact HDF5 dataset");
@@ -355,9 +359,12 @@ class File {
         // chunked
         const int rank = (int)d.s.dims.size();
         if ((int)d.lay.chunk.size() != rank) fail_io("HDF5 chunk rank does not match the dataspace");
-        std::vector<uint8_t> out(bytes, 0);
         uint64_t cbytes = es;
-        for (uint64_t c : d.lay.chunk) cbytes *= c;
+        for (uint64_t c : d.lay.chunk) {
+            if (c == 0 || c > (1ull << 31) / cbytes) fail_io("bad HDF5 chunk dimensions");
+            cbytes *= c;
+        }
+        std::vector<uint8_t> out(bytes, 0);
         auto place = [&](const std::vector<uint64_t>& off, std::vector<uint8_t> chunk, uint32_t mask) {
             chunk = unfilter(std::move(chunk), d.filters, mask, cbytes);
             if (chunk.size() < cbytes) fail_io("short HDF5 chunk");
@@ -375,6 +382,8 @@ class File {
                 }
                 if (inside && off[rank - 1] < d.s.dims[rank - 1]) {
                     const uint64_t cnt = std::min<uint64_t>(last, d.s.dims[rank - 1] - off[rank - 1]);
+                    if (dst > n || cnt > n - dst || (src + cnt) * es > chunk.size())
+                        fail_io("HDF5 chunk outside its dataset");
                     memcpy(out.data() + dst * es, chunk.data() + src * es, cnt * es);
                 }
                 int k = rank - 2;
@@ -393,7 +402,8 @@ class File {
             return out;
         }
         if (d.lay.addr == kUndef) return out;
-        walk_chunks(d.lay.addr, rank + 1, place, 0);
+        uint64_t budget = 1u << 20;  // B-tree nodes and chunks visited, against corrupt cycles
+        walk_chunks(d.lay.addr, rank + 1, place, 0, &budget);
         return out;
     }
 
@@ -663,8 +673,9 @@ class File {
     }
 
     template <class Place>
-    void walk_chunks(uint64_t node, int nkey, Place& place, int depth) const {
+    void walk_chunks(uint64_t node, int nkey, Place& place, int depth, uint64_t* budget) const {
         if (depth > 64) fail_io("HDF5 chunk B-tree too deep");
+        if ((*budget)-- == 0) fail_io("HDF5 chunk B-tree visits too many nodes");
         const uint64_t hdr = 8 + 2 * (uint64_t)so_;
         const std::vector<uint8_t> h = read(node, hdr);
         if (memcmp(h.data(), "TREE", 4) != 0 || h[4] != 1) fail_io("bad HDF5 chunk B-tree node");
@@ -680,8 +691,12 @@ class File {
             for (int k = 0; k < nkey; ++k) off.push_back(c.u(8));
             off.pop_back();
             const uint64_t kid = c.u(so_);
-            if (level > 0) walk_chunks(kid, nkey, place, depth + 1);
-            else place(off, read(kid, csize), mask);
+            if (level > 0) {
+                walk_chunks(kid, nkey, place, depth + 1, budget);
+            } else {
+                if ((*budget)-- == 0) fail_io("HDF5 chunk B-tree visits too many chunks");
+                place(off, read(kid, csize), mask);
+            }
         }
     }
 };

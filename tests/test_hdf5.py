@@ -206,3 +206,55 @@ def test_driver_reports_a_missing_hdf_template(tmp_path):
                        timeout=600)
     assert r.returncode != 0
     assert "/MDF/images/%d" % (len(stack) - 1) in r.stderr
+
+
+_FUZZ = r"""
+import ctypes as C, os, resource, sys
+import numpy as np
+sys.path.insert(0, os.path.dirname(sys.argv[1]))
+import _hdf5_writer as W
+resource.setrlimit(resource.RLIMIT_AS, (4 << 30, 4 << 30))
+lib = C.CDLL(sys.argv[2])
+rng = np.random.default_rng(11)
+d = sys.argv[3]
+imgs = [rng.standard_normal((12, 10)).astype(np.float32) for _ in range(5)]
+files = []
+p = os.path.join(d, "a.hdf"); W.write_eman2(p, imgs, snod_capacity=2, btree_capacity=3); files.append(p)
+p = os.path.join(d, "b.hdf")
+W.write_eman2(p, imgs, superblock=2, dataset_options={1: {"chunks": (5, 4), "filters": ("shuffle", "deflate")},
+                                                     2: {"compact": True}})
+files.append(p)
+p = os.path.join(d, "c.hdf"); W.write_eman1(p, imgs); files.append(p)
+base = [open(f, "rb").read() for f in files]
+seen = set()
+for it in range(900):
+    b = bytearray(base[it % 3])
+    for _ in range(int(rng.integers(1, 8))):
+        b[int(rng.integers(8, len(b)))] = int(rng.integers(0, 256))
+    q = os.path.join(d, "m.hdf")
+    open(q, "wb").write(bytes(b))
+    data = C.POINTER(C.c_float)(); nx, ny, nz = C.c_int(), C.c_int(), C.c_int()
+    err = C.create_string_buffer(256)
+    for idx in (0, 1, 3):
+        r = lib.gs_hdf_read_image(q.encode(), idx, C.byref(data), C.byref(nx), C.byref(ny), C.byref(nz), err, 256)
+        seen.add(r)
+        if r == 0:
+            lib.gs_host_free(data)
+print(sorted(seen))
+"""
+
+
+def test_corrupt_files_fail_cleanly(tmp_path):
+    # 900 files with random bytes overwritten (seeded), each read at three
+    # indexes in a child process under a 4 GB address-space limit: every read
+    # returns a status (no crash, no hang, no runaway allocation)
+    import ast
+    import subprocess
+    import sys
+    here = os.path.abspath(__file__)
+    r = subprocess.run([sys.executable, "-c", _FUZZ, here, LIB, str(tmp_path)], capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    seen = ast.literal_eval(r.stdout.strip().splitlines()[-1])
+    assert set(seen) <= {G.GS_OK, G.GS_ERR_IO, G.GS_ERR_UNSUPPORTED, G.GS_ERR_OOM}
+    assert G.GS_OK in seen and G.GS_ERR_IO in seen
