@@ -192,10 +192,10 @@ __device__ __forceinline__ void l2_discard128(const void* p) {
 }
 
 template <int N2, int V>
-__device__ __forceinline__ void corr_row_tile(const CorrArgs& a, int u, int t, float2* tile, const float2* twt) {
+__device__ __forceinline__ void corr_row_tile(const CorrArgs& a, int u, int t, float2* tile, const float2* twt,
+                                              int2 wp) {
     using F = CorrCfg<N2, V>;
     constexpr int L = F::L;
-    const int2 wp = a.unit_wp[u];
     const float2* Wr = a.W + (long long)wp.x * a.L2;
     const float2* Pr = a.P + (long long)wp.y * a.L2;
     float2* Rs = a.R + (long long)(u % a.S) * a.L2;
@@ -375,6 +375,17 @@ __device__ __forceinline__ const int* corr_dep(const CorrArgs& a, int item) {
     return (u >= 0 && u < a.nu) ? a.done_rows + u : nullptr;
 }
 
+// (window, pair) of the unit whose row tile `item` is ({0, 0} for column
+// tiles and the padding items past the last unit).  unit_wp is written by the
+// host before the launch, so this load needs no ordering.
+template <int N2, int V>
+__device__ __forceinline__ int2 corr_item_wp(const CorrArgs& a, int item, int total) {
+    using C = CorrCfg<N2, V>;
+    if (item >= total) return make_int2(0, 0);
+    const int s = item / (2 * C::T), j = item - s * (2 * C::T);
+    return (j < C::T && s < a.nu) ? __ldg(a.unit_wp + s) : make_int2(0, 0);
+}
+
 // Per-tile protocol: each warp checks the dependency of `item` before
 // working on it.
 template <int N2, int V>
@@ -455,7 +466,7 @@ __global__ void __launch_bounds__(CorrCfg<N2, V>::kThreads, CorrCfg<N2, V>::kCta
             if (threadIdx.x == 0) nxt = atomicAdd(a.next_item, 1);  // consumed after the tile
             const int s = item / (2 * F::T), j = item - s * (2 * F::T);
             if (j < F::T) {
-                if (s < a.nu) corr_row_tile<N2, V>(a, s, j, tile, twt);
+                if (s < a.nu) corr_row_tile<N2, V>(a, s, j, tile, twt, a.unit_wp[s]);
             } else {
                 const int u = s - a.lag;
                 if (u >= 0 && u < a.nu) corr_col_tile<N2, V>(a, u, j - F::T, tile, twt, ymask);
@@ -483,10 +494,13 @@ __global__ void __launch_bounds__(CorrCfg<N2, V>::kThreads, CorrCfg<N2, V>::kCta
     __syncthreads();
     int item = ish[0];
     for (int iter = 0; item < total; ++iter) {
+        // the unit's (window, pair) is read-only in this launch: its load is
+        // issued before the dependency wait and overlaps it
+        const int2 wp = corr_item_wp<N2, V>(a, item, total);
         corr_wait_for<N2, V>(a, item);
         const int s = item / (2 * F::T), j = item - s * (2 * F::T);
         if (j < F::T) {
-            if (s < a.nu) corr_row_tile<N2, V>(a, s, j, tile, twt);
+            if (s < a.nu) corr_row_tile<N2, V>(a, s, j, tile, twt, wp);
         } else {
             const int u = s - a.lag;
             if (u >= 0 && u < a.nu) corr_col_tile<N2, V>(a, u, j - F::T, tile, twt, ymask);
