@@ -671,7 +671,11 @@ def main() -> int:
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
-        line = run_reference(args, rank, world)
+        try:
+            line = run_reference(args, rank, world)
+        except Exception as e:  # a failed reference run is reported, not raised
+            line = {"impl": "reference",
+                    "unavailable": "reference run failed: %s" % " ".join(str(e).split())[:300]}
     else:
         if world > 1:
             import datetime
