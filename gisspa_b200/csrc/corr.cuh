@@ -20,8 +20,10 @@
 // barrier that ends a tile, one thread (the publisher, the CTA's last thread,
 // which has the lightest share of step 1 when the tasks do not divide evenly)
 // increments the unit's counter, so a pass of a unit is done at T
-// increments, and each warp checks the dependency of its CTA's next item
-// itself before starting it.  Per warp: every warp counts its own share
+// increments, claims the CTA's next-but-one item (written into the CTA's
+// ring of claimed items just before the following barrier, so its warp does
+// not wait for the atomic), and each warp checks the dependency of its CTA's
+// next item itself before starting it.  Per warp: every warp counts its own share
 // before that barrier (a pass is done at warps x T increments), and thread 0
 // waits for the next item's dependency before it.  Both dependencies point at
 // items that come earlier in the claim order, and an item is claimed only by
@@ -493,6 +495,7 @@ __global__ void __launch_bounds__(CorrCfg<N2, V>::kThreads, CorrCfg<N2, V>::kCta
     }
     __syncthreads();
     int item = ish[0];
+    int claimed = 0;  // the publisher's claim for slot (iter + 1) & 3, made after the previous barrier
     for (int iter = 0; item < total; ++iter) {
         // the unit's (window, pair) is read-only in this launch: its load is
         // issued before the dependency wait and overlaps it
@@ -505,15 +508,18 @@ __global__ void __launch_bounds__(CorrCfg<N2, V>::kThreads, CorrCfg<N2, V>::kCta
             const int u = s - a.lag;
             if (u >= 0 && u < a.nu) corr_col_tile<N2, V>(a, u, j - F::T, tile, twt, ymask);
         }
+        // the claim made after the previous barrier enters the ring only now,
+        // so the publisher's warp did not wait for the atomic's return
+        if (threadIdx.x == kPub && iter > 0) ish[(iter + 1) & 3] = claimed;
         // every thread is done with the item: the tile buffer is free, the
         // item's stores and atomics are ordered before its publication, and
-        // slot (iter + 1) & 3 (written two barriers ago) holds the next item;
-        // slot (iter + 2) & 3 was last read two iterations ago
+        // slot (iter + 1) & 3 holds the next item; slot (iter + 2) & 3 was
+        // last read two iterations ago
         __syncthreads();
         const int next = ish[(iter + 1) & 3];
         if (threadIdx.x == kPub) {
             corr_publish<N2, V>(a, item);
-            ish[(iter + 2) & 3] = atomicAdd(a.next_item, 1);
+            claimed = atomicAdd(a.next_item, 1);  // for slot (iter + 2) & 3
         }
         item = next;
     }
