@@ -75,12 +75,16 @@ class Node:
 
 
 class Writer:
-    def __init__(self, superblock=0, userblock=0, snod_capacity=8, btree_capacity=32, dense_links=False):
+    def __init__(self, superblock=0, userblock=0, snod_capacity=8, btree_capacity=32, dense_links=False,
+                 header_messages=None):
         self.sb = superblock
         self.userblock = userblock
         self.snod_cap = snod_capacity
         self.bt_cap = btree_capacity
         self.dense_links = dense_links
+        # at most this many messages per header block; the rest go to chained
+        # continuation blocks (as libhdf5 does when attributes keep being added)
+        self.per_block = header_messages
         self.buf = bytearray()
 
     def _alloc(self, b):
@@ -90,12 +94,31 @@ class Writer:
         return addr
 
     # -- object headers -------------------------------------------------
-    def _header(self, msgs):
+    def _msgs(self, msgs):
         if self.sb >= 2:
-            body = b"".join(struct.pack("<BHB", t, len(d), 0) + d for t, d in msgs)
+            return b"".join(struct.pack("<BHB", t, len(d), 0) + d for t, d in msgs)
+        return b"".join(struct.pack("<HHB3x", t, len(_pad8(d)), 0) + _pad8(d) for t, d in msgs)
+
+    def _header(self, msgs):
+        n_all = len(msgs)
+        k = self.per_block
+        if k and len(msgs) > k:
+            # chain: the last block first, each earlier block ending with a
+            # continuation message (address, length) to the next
+            blocks = [msgs[i:i + k] for i in range(0, len(msgs), k)]
+            nxt = None
+            for blk in reversed(blocks[1:]):
+                blk = list(blk) + ([nxt] if nxt else [])
+                body = self._msgs(blk)
+                raw = (b"OCHK" + body + b"\0" * 4) if self.sb >= 2 else body
+                addr = self._alloc(raw)
+                nxt = (0x10, struct.pack("<QQ", addr, len(raw)))
+                n_all += 1
+            msgs = list(blocks[0]) + [nxt]
+        body = self._msgs(msgs)
+        if self.sb >= 2:
             return self._alloc(b"OHDR" + struct.pack("<BBI", 2, 2, len(body)) + body + b"\0" * 4)
-        body = b"".join(struct.pack("<HHB3x", t, len(_pad8(d)), 0) + _pad8(d) for t, d in msgs)
-        return self._alloc(struct.pack("<BBHII4x", 1, 0, len(msgs), 1, len(body)) + body)
+        return self._alloc(struct.pack("<BBHII4x", 1, 0, n_all, 1, len(body)) + body)
 
     def _attr_msgs(self, attrs):
         out = []

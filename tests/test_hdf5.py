@@ -71,6 +71,24 @@ def test_eman2_layout_round_trip(tmp_path, superblock):
     assert e.value.status == G.GS_ERR_IO
 
 
+@pytest.mark.parametrize("superblock", [0, 2])
+def test_attributes_in_continuation_blocks(tmp_path, superblock):
+    # EMAN2 puts dozens of attributes on every image group; libhdf5 then
+    # spreads the group's object header over chained continuation blocks
+    rng = np.random.default_rng(8)
+    imgs = _images(rng, 2, (9, 14))
+    extra = {"EMAN.attr%02d" % k: np.float32(k + 0.5) for k in range(40)}
+    extra["EMAN.micrograph_id"] = "mic_0001"
+    extra["EMAN.orientation"] = np.arange(3, dtype=np.float32)
+    p = str(tmp_path / "cont.hdf")
+    W.write_eman2(p, imgs, attrs={0: extra, 1: extra}, superblock=superblock, header_messages=5)
+    for n, im in enumerate(imgs):
+        assert np.array_equal(G.read_hdf_image(p, n), im)
+    assert float(G.read_hdf_attribute(p, "/MDF/images/1", "EMAN.attr39")[0]) == 39.5
+    assert G.read_hdf_attribute(p, "/MDF/images/0", "EMAN.micrograph_id") == "mic_0001"
+    assert np.array_equal(G.read_hdf_attribute(p, "/MDF/images/0", "EMAN.orientation"), [0.0, 1.0, 2.0])
+
+
 def test_many_images_across_symbol_nodes_and_btree_levels(tmp_path):
     # two names per symbol-table node and three children per B-tree node:
     # 23 images need 12 leaves, 4 level-1 nodes, 2 level-2 nodes and a root
