@@ -193,7 +193,7 @@ def cpu_baseline(ds, kw, geom) -> dict:
                  padding_size=kw["window"], phase_flip=1, overlap=kw["overlap"])
     ctf = O.make_ctf(p, m.defocus, m.dfdiff, m.dfang, kw["window"])
     l = geom.l
-    nt_s = 4
+    nt_s = min(16, ds.templates.shape[0])
     t0 = time.perf_counter()
     img = O.preprocess_micrograph(m.image, p, ctf, workers=cores)
     offx = O.window_offsets(img.shape[1], l, p.overlap)
@@ -208,7 +208,7 @@ def cpu_baseline(ds, kw, geom) -> dict:
     t_spec = (time.perf_counter() - t0) / nt_s
     chk = O.checker(l).astype(np.complex64)
     TSc = np.conj(TS) * chk[None]
-    nw_s = min(8, W.shape[0])
+    nw_s = W.shape[0]  # every window: 16 x 88 units at the full-size workload
     t0 = time.perf_counter()
     for w in range(nw_s):
         cc = O._ifft2_unnorm(W[w][None] * TSc, cores).real
