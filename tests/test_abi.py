@@ -51,3 +51,30 @@ def test_driver_help_runs_without_gpu():
         build.build_driver()
     r = subprocess.run([G.DRIVER_PATH, "-h"], capture_output=True, text=True)
     assert r.returncode == 0 and "config" in r.stdout
+
+
+_HAS_GPU_DEVICE = os.path.exists("/dev/nvidiactl") or os.path.exists("/dev/nvidia0")
+
+
+@pytest.mark.skipif(_HAS_GPU_DEVICE, reason="a GPU is present: the no-GPU failure path cannot be shown here")
+def test_no_gpu_is_an_error_not_a_fallback(tmp_path):
+    # without a CUDA device the library refuses to work (no CPU fallback):
+    # context creation returns GS_ERR_CUDA, the Python binding raises, and the
+    # drop-in driver exits non-zero after reading its inputs
+    import ctypes as C
+    import _helpers as H
+    lib = G.load_library()
+    h = C.c_void_p()
+    assert lib.gs_ctx_create(0, C.byref(h)) == G.GS_ERR_CUDA
+    with pytest.raises(G.GisspaError) as e:
+        G.Context(0)
+    assert e.value.status == G.GS_ERR_CUDA
+    if not os.path.exists(G.DRIVER_PATH):
+        from gisspa_b200 import build
+        build.build_driver()
+    H.materialize("small_pf1_all", str(tmp_path))
+    r = subprocess.run([G.DRIVER_PATH, "config"], cwd=str(tmp_path), capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode != 0
+    assert "CUDA" in r.stderr or "cuda" in r.stderr
+    assert not (tmp_path / "picks.lst").exists() or (tmp_path / "picks.lst").read_text() == ""
