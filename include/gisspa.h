@@ -123,7 +123,10 @@ int gs_version(void);
 int gs_params_default(gs_params* p);
 
 /* Context on one CUDA device; replaces main.cu:1071 cudaSetDevice + the
- * stream of main.cu:274.  Owns a stream and all device buffers. */
+ * stream of main.cu:274.  Owns a stream and all device buffers.  Opaque to
+ * callers: declared here so that C and C++ callers name one type. */
+struct gs_ctx;
+typedef struct gs_ctx gs_ctx;
 int gs_ctx_create(int device, struct gs_ctx** out);
 int gs_ctx_destroy(struct gs_ctx* ctx);
 /* Last error text of this context ("" if none). */

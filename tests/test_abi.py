@@ -78,3 +78,32 @@ def test_no_gpu_is_an_error_not_a_fallback(tmp_path):
     assert r.returncode != 0
     assert "CUDA" in r.stderr or "cuda" in r.stderr
     assert not (tmp_path / "picks.lst").exists() or (tmp_path / "picks.lst").read_text() == ""
+
+
+def test_header_is_plain_c(tmp_path):
+    # a C caller (the way a reference-side program would bind the library)
+    # compiles and links against include/gisspa.h with strict C99
+    import shutil
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc not available")
+    if not os.path.exists(G.LIB_PATH):
+        from gisspa_b200 import build
+        build.build_library()
+    src = tmp_path / "caller.c"
+    src.write_text(
+        '#include "gisspa.h"\n'
+        "int main(void) {\n"
+        "    gs_ctx* ctx = 0;\n"
+        "    gs_params p;\n"
+        "    float* img = 0; int nx, ny, nz; char err[64];\n"
+        "    gs_params_default(&p);\n"
+        "    if (gs_ctx_create(0, &ctx) == GS_OK) gs_ctx_destroy(ctx);\n"
+        "    if (gs_hdf_read_image(\"x.hdf\", 0, &img, &nx, &ny, &nz, err, sizeof err) == GS_OK) gs_host_free(img);\n"
+        "    return 0;\n"
+        "}\n")
+    libdir = os.path.dirname(G.LIB_PATH)
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror",
+                        "-I" + os.path.join(ROOT, "include"), str(src), "-L" + libdir, "-lgisspa_b200",
+                        "-Wl,-rpath," + libdir, "-o", str(tmp_path / "caller")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
