@@ -235,8 +235,8 @@ DTYPES = {"fp32": "f32", "tc-bf16": "bf16 hi+lo split, f32 accumulate",
 
 
 # DRAM bytes (read + write) of one persistent-kernel launch at window 720 per
-# (window, pair) unit, from an ncu capture of 88 windows x 100 pairs
-# (profiles/k_corr_persistent_l720_100pairs.md), scaled by units in the bench
+# (window, pair) unit, from an ncu capture of 88 windows x 100 pairs (10.59 GB
+# read + 0.11 GB written for 8800 units), scaled by units in the bench
 TRAFFIC_PER_PAIR_UNIT_L720 = (10585217280 + 106544128) / 8800.0
 
 
@@ -503,9 +503,8 @@ def run_ours(args, rank, world, local_rank):
         kname = ("k_corr_persistent (row + column tiles of one angle)" if args.precision == "fp32" else
                  "k_corr_tc (row + column tiles of one angle; N2-point DFT stage on the tensor cores)")
         # DRAM traffic of the persistent FP32 kernel per (window, pair) unit at
-        # l = 720, from one ncu capture of a 100-pair launch
-        # (profiles/k_corr_persistent_l720_100pairs.md: 10.50 GB read + 0.06 GB
-        # written for 8800 units), scaled to this launch's units
+        # l = 720, from one ncu capture of a 100-pair launch, scaled to this
+        # launch's units
         traffic = (TRAFFIC_PER_PAIR_UNIT_L720 * npairs * nw
                    if (l == 720 and args.precision == "fp32") else None)
         roof = {"bound": "fp32", "kernel": kname,

@@ -28,6 +28,8 @@ GS_ERR_ARG, GS_ERR_OOM, GS_ERR_CUDA, GS_ERR_STATE, GS_ERR_UNSUPPORTED, GS_ERR_TI
 STATUS = {0: "ok", 1: "invalid argument", 2: "out of memory", 3: "CUDA error",
           4: "invalid call order", 5: "unsupported input", 6: "device wait timed out",
           7: "I/O error"}
+# arithmetic of the correlation's DFT stages (gs_params.precision)
+GS_PREC_FP32, GS_PREC_TC_BF16, GS_PREC_TC_FP16 = 0, 1, 2
 
 
 class GsParams(C.Structure):

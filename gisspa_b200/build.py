@@ -15,6 +15,7 @@ import glob
 import os
 import subprocess
 import sys
+from typing import Optional
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -77,30 +78,33 @@ def build_merge_cli(force: bool = False) -> str:
     return MERGE
 
 
-def build_reference_checker() -> bool:
-    """Compile the reference's own sources into oracle/_ref (test
+def build_reference_checker(ref: Optional[str] = None) -> bool:
+    """Compile the reference's own sources (directory `ref`, or the
+    GISSPA_REFERENCE environment variable) into oracle/_ref (test
     infrastructure) when they are present on this machine."""
-    ref = os.environ.get("GISSPA_REFERENCE", "/root/reference")
-    if not os.path.isdir(ref):
+    ref = ref or os.environ.get("GISSPA_REFERENCE")
+    if not ref or not os.path.isdir(ref):
         return False
     _run(["make", "-C", os.path.join(ROOT, "oracle"), "ref", "REF=" + ref])
     return True
 
 
-def build_all(force: bool = False, reference: bool = True) -> None:
+def build_all(force: bool = False, reference: Optional[str] = None) -> None:
+    """Library, drop-in driver and merge CLI; the reference checker too when
+    `reference` (or GISSPA_REFERENCE) names the reference's source tree."""
     build_library(force)
     build_driver(force)
     build_merge_cli(force)
-    if reference:
-        build_reference_checker()
+    build_reference_checker(reference)
 
 
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
-    ap.add_argument("--no-reference", action="store_true")
+    ap.add_argument("--reference", default=None,
+                    help="reference source tree to build the parity checker from (default: $GISSPA_REFERENCE)")
     a = ap.parse_args()
-    build_all(a.force, not a.no_reference)
+    build_all(a.force, a.reference)
     return 0
 
 

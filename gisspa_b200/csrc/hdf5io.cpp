@@ -307,7 +307,15 @@ class File {
             c.skip(pad(tlen));
             a.s = space(c.at(slen), slen);
             c.skip(pad(slen));
-            const uint64_t bytes = a.t.cls >= 0 ? a.s.count() * (uint64_t)a.t.size : 0;
+            // the element count is bounded by the bytes left in the message
+            // before it is multiplied (a corrupt dataspace can claim 2^62)
+            uint64_t bytes = 0;
+            if (a.t.cls >= 0 && a.t.size > 0) {
+                const uint64_t left = m.data.size() - c.p;
+                const uint64_t n = a.s.count();
+                if (n > left / (uint64_t)a.t.size) fail_io("HDF5 attribute " + name + " runs past its message");
+                bytes = n * (uint64_t)a.t.size;
+            }
             a.raw.assign(c.at(bytes), c.at(bytes) + bytes);
             out[name] = std::move(a);
         }
@@ -770,6 +778,12 @@ int report_oom(char* err, size_t err_len) {
     if (err && err_len) snprintf(err, err_len, "out of host memory");
     return GS_ERR_OOM;
 }
+// any other exception (e.g. std::length_error) must not leave an extern "C"
+// function: it is reported as an unreadable file
+int report_other(const std::exception& e, char* err, size_t err_len) {
+    if (err && err_len) snprintf(err, err_len, "HDF5 read failed: %s", e.what());
+    return GS_ERR_IO;
+}
 
 }  // namespace
 
@@ -849,6 +863,8 @@ extern "C" int gs_hdf_read_image(const char* path, int index, float** host_data,
         return report(e, err, err_len);
     } catch (const std::bad_alloc&) {
         return report_oom(err, err_len);
+    } catch (const std::exception& e) {
+        return report_other(e, err, err_len);
     }
 }
 
@@ -878,6 +894,8 @@ extern "C" int gs_hdf_read_dataset(const char* path, const char* name, double** 
         return report(e, err, err_len);
     } catch (const std::bad_alloc&) {
         return report_oom(err, err_len);
+    } catch (const std::exception& e) {
+        return report_other(e, err, err_len);
     }
 }
 
@@ -916,6 +934,8 @@ extern "C" int gs_hdf_read_attribute(const char* path, const char* object, const
         return report(e, err, err_len);
     } catch (const std::bad_alloc&) {
         return report_oom(err, err_len);
+    } catch (const std::exception& e) {
+        return report_other(e, err, err_len);
     }
 }
 

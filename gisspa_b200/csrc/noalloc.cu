@@ -13,6 +13,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <map>
 #include <mutex>
 #include <type_traits>
 #include <utility>
@@ -38,29 +39,67 @@ constexpr size_t kTwBytes = 64u << 10;
 constexpr size_t kAccBytes = 1u << 20;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
-void* g_scratch_addr[kMaxDevices] = {nullptr};
+// Device addresses of the scratch array, one per CUDA context.  The module
+// holding the array is loaded once per context, so a context created anew
+// (e.g. the primary context after cudaDeviceReset) has a new address: the
+// cache is keyed by the context's unique ID, not by the device ordinal.
+std::map<unsigned long long, void*> g_scratch_addr;
 std::mutex g_scratch_mu;
 
-// Device address of the scratch array for the current device.  The host-side
-// name g_noalloc_scratch is only a stand-in symbol, so the address is looked
-// up once per device, with that device current.
+// Unique ID of the calling thread's current context (driver API, reached
+// through the runtime so that the library needs no libcuda link), or 0 when
+// no context is current or the driver cannot tell.
+unsigned long long current_context_id() {
+    using GetCurrent = int (*)(void**);
+    using GetId = int (*)(void*, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(f);
+        f = nullptr;
+        q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(f);
+        cudaGetLastError();
+    });
+    void* ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+    return id;
+}
+
+// Device address of the scratch array in the current context.  The
+// host-side name g_noalloc_scratch is only a stand-in symbol, so the address
+// is looked up with cudaGetSymbolAddress once per context (the first call in
+// a context; that lookup also makes the device's primary context current if
+// no runtime call has yet in this thread).
 int scratch_for_current_device(unsigned char** out) {
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    if (cudaGetDevice(&dev) != cudaSuccess) {
         cudaGetLastError();
         return GS_ERR_CUDA;
     }
     std::lock_guard<std::mutex> lk(g_scratch_mu);
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
-            cudaGetLastError();
-            return GS_ERR_CUDA;
-        }
-        g_scratch_addr[dev] = p;
+    unsigned long long id = current_context_id();
+    auto it = id ? g_scratch_addr.find(id) : g_scratch_addr.end();
+    if (it != g_scratch_addr.end()) {
+        *out = static_cast<unsigned char*>(it->second);
+        return GS_OK;
     }
-    *out = static_cast<unsigned char*>(g_scratch_addr[dev]);
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+        cudaGetLastError();
+        return GS_ERR_CUDA;
+    }
+    if (!id) id = current_context_id();  // the lookup may have made the context current
+    if (id) g_scratch_addr[id] = p;      // without an ID nothing is cached: looked up every call
+    *out = static_cast<unsigned char*>(p);
     return GS_OK;
 }
 

@@ -360,13 +360,15 @@ void gs_host_free(void* p);
  *                      this window, as gs_get_units reports them.
  * The intermediate maps, accumulators and twiddles live in one static device
  * array of GS_NOALLOC_SCRATCH_BYTES that every GPU loading this library holds
- * until process exit; l is limited to GS_NOALLOC_MAX_WINDOW (larger windows,
- * odd l, or l with too many prime factors return GS_ERR_UNSUPPORTED).
- * Work is queued on `stream` (a cudaStream_t, NULL = default stream) and the
- * call returns without waiting.  The first call on a device looks up the
- * array's device address and must come before any stream capture.  All calls
- * share the array and it keeps the last call's contents: calls that overlap
- * on the GPU (other streams, other host threads) race. */
+ * until process exit; l is limited to GS_NOALLOC_MAX_WINDOW (odd l returns
+ * GS_ERR_ARG; larger windows or l with too many prime factors return
+ * GS_ERR_UNSUPPORTED).  Work is queued on `stream` (a cudaStream_t, NULL =
+ * default stream) and the call returns without waiting.  The first call in
+ * each CUDA context (per device, and again after that context is destroyed
+ * and re-created, e.g. by cudaDeviceReset) looks up the array's device
+ * address and must come before any stream capture.  All calls share the
+ * array and it keeps the last call's contents: calls that overlap on the GPU
+ * (other streams, other host threads) race. */
 #define GS_NOALLOC_SCRATCH_BYTES (32u << 20)
 #define GS_NOALLOC_MAX_WINDOW 2012
 int gs_correlate_window_noalloc(const float* d_window_spectrum, const float* d_pair_spectra,

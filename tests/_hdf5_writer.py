@@ -49,6 +49,14 @@ def _space_msg(shape):
     return struct.pack("<BBBB4x", 1, len(shape), 0, 0) + b"".join(struct.pack("<Q", d) for d in shape)
 
 
+class ClaimedShape:
+    """An attribute whose dataspace claims `shape` while only `data` is
+    stored (a corrupt file: the claimed size need not fit the message)."""
+
+    def __init__(self, dtype, shape, data):
+        self.dtype, self.shape, self.data = np.dtype(dtype), tuple(shape), bytes(data)
+
+
 class Node:
     """A group (children by name) or a dataset, with attributes."""
 
@@ -123,7 +131,9 @@ class Writer:
     def _attr_msgs(self, attrs):
         out = []
         for name, val in attrs.items():
-            if isinstance(val, str):
+            if isinstance(val, ClaimedShape):
+                dt, shape, data = _dtype_msg(val.dtype), val.shape, val.data
+            elif isinstance(val, str):
                 raw = val.encode() + b"\0"
                 dt, shape, data = _dtype_msg("S%d" % len(raw)), (), raw
             else:

@@ -2,9 +2,12 @@
 200^2, 72 angles, window 720, overlap 200: 12.67 M units) on a subset of
 units, against the FP64 oracle: every unit of a few seeded (template, angle)
 pairs in all 88 windows, plus seeded units among those whose score reaches the
-pick threshold.  Scores within SCORE_RTOL; positions equal unless the oracle's
-own map holds a value within 1e-5 of its peak at the GPU's position (a tie at
-FP32 resolution).  GISSPA_SLOW=1 widens the subset about four-fold."""
+pick threshold.  Run for the FP32 path (scores within SCORE_RTOL) and for both
+tensor-core precisions (split BF16 and split FP16 DFT stage, scores within
+TC_SCORE_RTOL, the bound stated for that path).  Positions equal unless the
+oracle's own map holds a value within 1e-5 of its peak at the GPU's position
+(a tie at FP32 resolution).  The oracle side is computed once and shared by
+the three precisions.  GISSPA_SLOW=1 widens the subset about four-fold."""
 import os
 
 import numpy as np
@@ -21,60 +24,106 @@ SLOW = os.environ.get("GISSPA_SLOW") == "1"
 N_PAIRS = 24 if SLOW else 6          # (template, angle) pairs, all windows each
 N_PICK_UNITS = 256 if SLOW else 64   # units at or above the threshold
 WORKERS = min(16, os.cpu_count() or 1)
+# score bound of the tensor-core path against FP64 (split 16-bit DFT stage)
+TC_SCORE_RTOL = 1e-3
+L = 720
+
+_CACHE = {}
 
 
-def test_full_size_units_match_oracle():
-    kw = synth.config_full(seed=1)
-    seed = kw.pop("seed")
-    ds = synth.make_dataset(seed, **kw)
-    m = ds.micrographs[0]
-    ctf = (m.defocus, m.dfdiff, m.dfang)
-    p = ds.params
-    gp = G.default_params(apix=float(p["angpix"]), phi_step=float(p["phistep"]), kk=float(p["kk"]),
-                          energy=float(p["energy"]), cs=float(p["cs"]), highres=float(p["Highres"]),
-                          lowres=float(p["Lowres"]), d_m=float(p["diameter"]), thres=float(p["threshold"]),
-                          window_size=int(p["window_size"]), overlap=int(p["overlap"]),
-                          phase_flip=int(p["phase_flip"]))
-    with G.Context(0) as ctx:
-        ctx.set_templates(gp, ds.templates, ctf)
-        ctx.search(m.image, ctf)
-        g = ctx.geometry(m.image.shape[1], m.image.shape[0])
-        na, nw, nt = g.n_angles, g.n_windows_x * g.n_windows_y, g.n_templates
-        u = ctx.units((na, nw, nt))
-    l = 720
-    assert (na, nw, nt) == (72, 88, 2000)
+def _dataset():
+    if "ds" not in _CACHE:
+        kw = synth.config_full(seed=1)
+        seed = kw.pop("seed")
+        _CACHE["ds"] = synth.make_dataset(seed, **kw)
+    return _CACHE["ds"]
 
+
+def _search_units(precision):
+    key = ("units", precision)
+    if key not in _CACHE:
+        ds = _dataset()
+        m = ds.micrographs[0]
+        ctf = (m.defocus, m.dfdiff, m.dfang)
+        p = ds.params
+        gp = G.default_params(apix=float(p["angpix"]), phi_step=float(p["phistep"]), kk=float(p["kk"]),
+                              energy=float(p["energy"]), cs=float(p["cs"]), highres=float(p["Highres"]),
+                              lowres=float(p["Lowres"]), d_m=float(p["diameter"]),
+                              thres=float(p["threshold"]), window_size=int(p["window_size"]),
+                              overlap=int(p["overlap"]), phase_flip=int(p["phase_flip"]))
+        gp.precision = precision
+        with G.Context(0) as ctx:
+            ctx.set_templates(gp, ds.templates, ctf)
+            ctx.search(m.image, ctf)
+            g = ctx.geometry(m.image.shape[1], m.image.shape[0])
+            shape = (g.n_angles, g.n_windows_x * g.n_windows_y, g.n_templates)
+            _CACHE[key] = ctx.units(shape)
+    return _CACHE[key]
+
+
+def _subset(u, thres):
+    """The seeded unit subset: fixed (template, angle) pairs over all windows
+    (drawn independently of the search) and units at or above the threshold
+    (drawn from the FP32 search's units)."""
+    na, nw, nt = u["score"].shape
     rng = np.random.default_rng(720)
     units = set()
     for J, ai in zip(rng.choice(nt, N_PAIRS, replace=False), rng.choice(na, N_PAIRS)):
         units.update((int(ai), w, int(J)) for w in range(nw))
-    hi = np.argwhere(np.isfinite(u["score"]) & (u["score"] >= float(p["threshold"])))
+    hi = np.argwhere(np.isfinite(u["score"]) & (u["score"] >= thres))
     assert len(hi) > 0
     for q in rng.choice(len(hi), min(N_PICK_UNITS, len(hi)), replace=False):
         units.add(tuple(int(x) for x in hi[q]))
-    units = sorted(units)
+    return sorted(units)
 
+
+def _oracle_units():
+    """FP64 maps' (score, pos, border-masked map) of every subset unit."""
+    if "oracle" in _CACHE:
+        return _CACHE["oracle"]
+    ds = _dataset()
+    m = ds.micrographs[0]
+    p = ds.params
+    ctf = (m.defocus, m.dfdiff, m.dfang)
+    u = _search_units(G.GS_PREC_FP32)
+    units = _subset(u, float(p["threshold"]))
     op = O.Params(apix=float(p["angpix"]), phi_step=float(p["phistep"]), kk=float(p["kk"]),
                   energy=float(p["energy"]), cs=float(p["cs"]), highres=float(p["Highres"]),
-                  lowres=float(p["Lowres"]), d_m=float(p["diameter"]), thres=0.0, padding_size=l,
+                  lowres=float(p["Lowres"]), d_m=float(p["diameter"]), thres=0.0, padding_size=L,
                   phase_flip=1, overlap=int(p["overlap"]))
-    octf = O.make_ctf(op, *ctf, l)
+    octf = O.make_ctf(op, *ctf, L)
     img = O.preprocess_micrograph(m.image, op, octf, workers=WORKERS)
-    offx = O.window_offsets(m.image.shape[1], l, op.overlap)
-    offy = O.window_offsets(m.image.shape[0], l, op.overlap)
-    W = O.window_spectra(O.split_windows(img, offx, offy, l), op, workers=WORKERS)
+    offx = O.window_offsets(m.image.shape[1], L, op.overlap)
+    offy = O.window_offsets(m.image.shape[0], L, op.overlap)
+    W = O.window_spectra(O.split_windows(img, offx, offy, L), op, workers=WORKERS)
     tids = sorted({J for _, _, J in units})
-    T = dict(zip(tids, O.prepare_templates(ds.templates[tids], op, l, octf, workers=WORKERS)))
+    T = dict(zip(tids, O.prepare_templates(ds.templates[tids], op, L, octf, workers=WORKERS)))
     angs = O.angle_list(op.phi_step)
-    chk = O.checker(l)
+    chk = O.checker(L)
+    border = O.border_mask(L, op.d_m)
     spec = {}
-    worst, ties, n = 0.0, 0, 0
+    res = {}
     for ai, w, J in units:
         if (ai, J) not in spec:
             spec[(ai, J)] = np.conj(O.template_spectra(T[J][None], angs[ai], op.d_m, workers=WORKERS)[0]) * chk
         cc = O._ifft2_unnorm((W[w] * spec[(ai, J)])[None], WORKERS).real
         st = O.score_maps(cc, op.d_m)
-        ref_s, ref_p = float(st.score[0]), int(st.pos[0])
+        masked = np.where(border, 0.0, cc[0]).ravel()
+        res[(ai, w, J)] = (float(st.score[0]), int(st.pos[0]), masked)
+    _CACHE["oracle"] = res
+    return res
+
+
+@pytest.mark.parametrize("precision,rtol", [(G.GS_PREC_FP32, H.SCORE_RTOL),
+                                            (G.GS_PREC_TC_BF16, TC_SCORE_RTOL),
+                                            (G.GS_PREC_TC_FP16, TC_SCORE_RTOL)],
+                         ids=["fp32", "tc_bf16", "tc_fp16"])
+def test_full_size_units_match_oracle(precision, rtol):
+    ref = _oracle_units()
+    u = _search_units(precision)
+    assert u["score"].shape == (72, 88, 2000)
+    worst, ties, n = 0.0, 0, 0
+    for (ai, w, J), (ref_s, ref_p, masked) in ref.items():
         got_s, got_p = float(u["score"][ai, w, J]), int(u["pos"][ai, w, J])
         assert np.isfinite(ref_s) == np.isfinite(got_s), (ai, w, J)
         if not np.isfinite(ref_s):
@@ -82,11 +131,10 @@ def test_full_size_units_match_oracle():
         n += 1
         worst = max(worst, abs(got_s - ref_s) / abs(ref_s))
         if got_p != ref_p:
-            masked = np.where(O.border_mask(l, op.d_m), 0.0, cc[0])
-            peak = masked.ravel()[ref_p]
-            assert masked.ravel()[got_p] >= peak - 1e-5 * abs(peak), (ai, w, J, got_p, ref_p)
+            peak = masked[ref_p]
+            assert masked[got_p] >= peak - 1e-5 * abs(peak), (ai, w, J, got_p, ref_p)
             ties += 1
-    print("full-size subset: %d units (%d pairs x %d windows + threshold units), worst score error %.2e, "
-          "%d near-tie positions" % (n, N_PAIRS, nw, worst, ties))
-    assert worst <= H.SCORE_RTOL, worst
+    print("full-size subset, precision %d: %d units (%d pairs x 88 windows + threshold units), "
+          "worst score error %.2e, %d near-tie positions" % (precision, n, N_PAIRS, worst, ties))
+    assert worst <= rtol, worst
     assert ties <= max(2, n // 100), ties

@@ -276,3 +276,18 @@ def test_corrupt_files_fail_cleanly(tmp_path):
     seen = ast.literal_eval(r.stdout.strip().splitlines()[-1])
     assert set(seen) <= {G.GS_OK, G.GS_ERR_IO, G.GS_ERR_UNSUPPORTED, G.GS_ERR_OOM}
     assert G.GS_OK in seen and G.GS_ERR_IO in seen
+
+
+def test_huge_attribute_dataspace_is_an_io_error(tmp_path):
+    # a dataspace of 2^31 x 2^31 doubles in an attribute message holding 8
+    # bytes: the element count overflows any byte count; the read must return
+    # GS_ERR_IO instead of sizing a buffer from it
+    rng = np.random.default_rng(5)
+    path = str(tmp_path / "huge_attr.hdf")
+    bad = W.ClaimedShape(np.float64, (2 ** 31, 2 ** 31), b"\0" * 8)
+    W.write_eman2(path, _images(rng, 1, (8, 8)), attrs={0: {"EMAN.bad": bad}})
+    for call in (lambda: G.read_hdf_attribute(path, "/MDF/images/0", "EMAN.bad"),
+                 lambda: G.read_hdf_image(path, 0)):
+        with pytest.raises(G.GisspaError) as e:
+            call()
+        assert e.value.status == G.GS_ERR_IO

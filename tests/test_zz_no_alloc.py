@@ -68,12 +68,21 @@ def test_noalloc_matches_search(l, overlap, tsize, nt):
     dev = torch.device("cuda", 0)
     d_P = torch.from_numpy(P.astype(np.complex64)).to(dev)
     d_units = torch.zeros((nt, 4), dtype=torch.float32, device=dev)
-    for call, w in enumerate((nw - 1, 0)):          # two calls in a row, different windows
-        d_W = torch.from_numpy(W[w].astype(np.complex64)).to(dev)
+    wins = (nw - 1, 0)                               # two calls in a row, different windows
+    d_Ws = [torch.from_numpy(W[w].astype(np.complex64)).to(dev) for w in wins]
+    free_after_first = None
+    for call, w in enumerate(wins):
         d_units.fill_(float("nan"))
         torch.cuda.synchronize()
-        G.correlate_window_noalloc(d_W.data_ptr(), d_P.data_ptr(), nt, l, d_m, d_units.data_ptr())
+        G.correlate_window_noalloc(d_Ws[call].data_ptr(), d_P.data_ptr(), nt, l, d_m, d_units.data_ptr())
         torch.cuda.synchronize()
+        # the first call may load the library's module (which holds the static
+        # scratch); from then on a call takes no device memory at all
+        free_now = torch.cuda.mem_get_info(dev)[0]
+        if call == 0:
+            free_after_first = free_now
+        else:
+            assert free_now == free_after_first, (free_after_first, free_now)
         got = d_units.cpu().numpy()
         score = got[:, 0]
         pos = got[:, 1].copy().view(np.int32)
