@@ -76,7 +76,8 @@ PICK_DTYPE = np.dtype([("angle_index", "<i4"), ("phi", "<f4"), ("window_x", "<i4
 # every entry point declared in include/gisspa.h
 EXPORTS = ("gs_status_string", "gs_version", "gs_params_default", "gs_ctx_create",
            "gs_ctx_destroy", "gs_ctx_last_error", "gs_set_templates", "gs_get_geometry",
-           "gs_search", "gs_search_device", "gs_get_units", "gs_picks_free", "gs_get_timings",
+           "gs_search", "gs_search_device", "gs_get_units", "gs_get_pixel_max", "gs_picks_free",
+           "gs_get_timings",
            "gs_get_stats", "gs_set_kernel_timing", "gs_set_option",
            "gs_correlate_window_noalloc", "gs_search_batch", "gs_get_tuning", "gs_score_grad",
            "gs_refine", "gs_merge_duplicates", "gs_hdf_read_image", "gs_hdf_read_dataset",
@@ -117,6 +118,7 @@ def load_library(path: Optional[str] = None) -> C.CDLL:
     lib.gs_search_device.argtypes = [vp, C.c_void_p, C.c_int, C.c_int, C.POINTER(GsCtf),
                                      C.POINTER(C.POINTER(GsPick)), C.POINTER(C.c_size_t)]
     lib.gs_get_units.argtypes = [vp, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]
+    lib.gs_get_pixel_max.argtypes = [vp, C.c_int, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.gs_picks_free.argtypes = [C.POINTER(GsPick)]
     lib.gs_picks_free.restype = None
     lib.gs_get_timings.argtypes = [vp, C.POINTER(C.c_float), C.c_int]
@@ -410,6 +412,19 @@ class Context:
         self._check(self._lib.gs_get_units(self._h, out.ctypes.data, n.value, C.byref(n)),
                     "gs_get_units")
         return out.reshape(shape) if shape is not None else out
+
+    def pixel_max(self, thres: float, shape: Tuple[int, int], micrograph: int = 0):
+        """Per-pixel maximum of cc / sigma over (template, angle) of micrograph
+        `micrograph` (shape (ny, nx)) of the last search (gs_get_pixel_max):
+        (value, template_index, angle_index) arrays; value 0 and indices -1
+        where no map reaches `thres`."""
+        ny, nx = shape
+        value = np.zeros((ny, nx), dtype=np.float32)
+        tmpl = np.zeros((ny, nx), dtype=np.int32)
+        ang = np.zeros((ny, nx), dtype=np.int32)
+        self._check(self._lib.gs_get_pixel_max(self._h, micrograph, thres, value.ctypes.data,
+                                               tmpl.ctypes.data, ang.ctypes.data), "gs_get_pixel_max")
+        return value, tmpl, ang
 
     def stats(self) -> GsStats:
         st = GsStats()

@@ -7,6 +7,7 @@ Outputs
   gisspa_b200/lib/libgisspa_b200.so   C ABI of include/gisspa.h (CUDA kernels)
   gisspa_b200/lib/gisspa_main         drop-in CLI for the reference's ./main
   gisspa_b200/lib/gisspa_merge        drop-in for its duplicate-merging script
+  gisspa_b200/lib/libgisspa_peak.so   FP32 FMA microbenchmark (bench.py's roofline peak)
 """
 from __future__ import annotations
 
@@ -58,6 +59,36 @@ def build_library(force: bool = False) -> str:
     return LIB
 
 
+PEAK = os.path.join(LIBDIR, "libgisspa_peak.so")
+
+
+def build_peak(force: bool = False) -> str:
+    """FP32 FMA microbenchmark used by bench.py for the roofline peak (not
+    part of the search's C ABI)."""
+    src = os.path.join(CSRC, "peak", "fma_peak.cu")
+    if not force and _newer(PEAK, [src]):
+        return PEAK
+    os.makedirs(LIBDIR, exist_ok=True)
+    _run([NVCC] + NVCC_FLAGS + ARCH + ["-shared", "-o", PEAK, src])
+    return PEAK
+
+
+CPU_BASELINE = os.path.join(ROOT, "oracle", "_cpu", "libgisspa_cpu.so")
+
+
+def build_cpu_baseline(force: bool = False) -> str:
+    """C++/OpenMP restatement of the correlation and scoring (oracle/cpu),
+    timed by bench.py as the CPU baseline; x86-64-v3 (AVX2 + FMA) so that it
+    runs on any current host."""
+    src = os.path.join(ROOT, "oracle", "cpu", "gisspa_cpu.cpp")
+    if not force and _newer(CPU_BASELINE, [src]):
+        return CPU_BASELINE
+    os.makedirs(os.path.dirname(CPU_BASELINE), exist_ok=True)
+    _run(["g++", "-O3", "-march=x86-64-v3", "-fopenmp", "-std=c++17", "-shared", "-fPIC", "-Wall",
+          "-o", CPU_BASELINE, src])
+    return CPU_BASELINE
+
+
 def build_driver(force: bool = False) -> str:
     dsrc = sorted(glob.glob(os.path.join(CSRC, "driver", "*.cpp")))
     deps = dsrc + glob.glob(os.path.join(CSRC, "driver", "*.hpp")) + [LIB, os.path.join(INCLUDE, "gisspa.h")]
@@ -85,7 +116,7 @@ def build_reference_checker(ref: Optional[str] = None) -> bool:
     ref = ref or os.environ.get("GISSPA_REFERENCE")
     if not ref or not os.path.isdir(ref):
         return False
-    _run(["make", "-C", os.path.join(ROOT, "oracle"), "ref", "REF=" + ref])
+    _run(["make", "-C", os.path.join(ROOT, "oracle"), "ref", "ref-default", "REF=" + ref])
     return True
 
 
@@ -95,6 +126,8 @@ def build_all(force: bool = False, reference: Optional[str] = None) -> None:
     build_library(force)
     build_driver(force)
     build_merge_cli(force)
+    build_peak(force)
+    build_cpu_baseline(force)
     build_reference_checker(reference)
 
 

@@ -10,6 +10,7 @@
 #include "fastfft.cuh"
 #include "kernels.cuh"
 #include "norm1.cuh"
+#include "pixmax.cuh"
 #include "tccorr.cuh"
 #include "refine.cuh"
 
@@ -65,6 +66,12 @@ struct gs_ctx {
     // last search
     int last_na = 0, last_nw = 0, last_nt = 0;
     bool have_units = false;
+    struct MicGeom {
+        int nx, ny, w0;
+        std::vector<int> offx, offy;
+    };
+    std::vector<MicGeom> last_mics;  // micrographs of the last norm_type 0 search
+    DBuf pix_keys, pix_pairs, pix_R;  // gs_get_pixel_max buffers
     float timings[GS_TIMING_COUNT] = {0, 0, 0, 0, 0, 0, 0, 0};
     bool kernel_timing = false;
     bool generic_fft = false;
@@ -1508,6 +1515,8 @@ static int search_many(gs_ctx* ctx, std::vector<MicPlan>& mics, std::vector<std:
         ctx->last_nw = NW;
         ctx->last_nt = N;
         ctx->have_units = true;
+        ctx->last_mics.clear();
+        for (const MicPlan& mp : mics) ctx->last_mics.push_back(gs_ctx::MicGeom{mp.nx, mp.ny, mp.w0, mp.offx, mp.offy});
         for (size_t m = 0; m < mics.size(); ++m) TRY(compact_picks(ctx, mics[m], NW, angles, &(*res)[m]));
     }
     CK(cudaEventRecord(ev[3], ctx->stream));
@@ -1519,6 +1528,107 @@ static int search_many(gs_ctx* ctx, std::vector<MicPlan>& mics, std::vector<std:
     memcpy(ctx->timings, t, sizeof t);
     ctx->counters.searches += 1;
     ctx->counters.units += (unsigned long long)total_units;
+    return GS_OK;
+}
+
+// Per-pixel maximum of cc / sigma over (angle, template) for micrograph `mic`
+// of the last search (pixmax.cuh): the units whose score reaches `thres` are
+// recomputed with the two-pass FP32 kernels, angle by angle, window by window.
+static int pixel_max_impl(gs_ctx* ctx, int mic, float thres, float* value, int* tmpl, int* angle_out) {
+    const gs_params& p = ctx->p;
+    const int l = ctx->l;
+    const long long l2 = (long long)l * l;
+    const int N = ctx->ntmpl, Np = (N + 1) / 2, NW = ctx->last_nw, na = ctx->last_na;
+    const gs_ctx::MicGeom& mg = ctx->last_mics[mic];
+    const int bx = (int)mg.offx.size(), nwm = bx * (int)mg.offy.size();
+    const std::vector<float> angles = angle_list(p.phi_step);
+    if ((int)angles.size() != na) return set_err(ctx, GS_ERR_STATE, "parameters changed since the search");
+    // this micrograph's units, every angle
+    std::vector<UnitOut> u((size_t)na * nwm * N);
+    for (int a = 0; a < na; ++a)
+        CK(cudaMemcpyAsync(u.data() + (size_t)a * nwm * N,
+                           P<UnitOut>(ctx->units) + ((size_t)a * NW + mg.w0) * N, sizeof(UnitOut) * (size_t)nwm * N,
+                           cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const size_t npix = (size_t)mg.nx * mg.ny;
+    TRY(ensure(ctx, ctx->pix_keys, sizeof(unsigned long long) * npix));
+    TRY(ensure(ctx, ctx->pix_pairs, sizeof(int) * Np));
+    const int chunk = (int)std::max<long long>(1, std::min<long long>(Np, (1ll << 30) / (l2 * (long long)sizeof(float2))));
+    TRY(ensure(ctx, ctx->pix_R, sizeof(float2) * l2 * chunk));
+    TRY(ensure(ctx, ctx->tspec, sizeof(float2) * l2 * Np));
+    TRY(ensure(ctx, ctx->pstats, sizeof(double) * 2 * N));
+    TRY(ensure(ctx, ctx->coef, sizeof(float4) * Np));
+    CK(cudaMemsetAsync(ctx->pix_keys.p, 0, sizeof(unsigned long long) * npix, ctx->stream));
+    unsigned long long* keys = P<unsigned long long>(ctx->pix_keys);
+    int* d_pairs = P<int>(ctx->pix_pairs);
+    float2* R = P<float2>(ctx->pix_R);
+    float2* TS = P<float2>(ctx->tspec);
+    const float2* W = P<float2>(ctx->win);
+    const float q_lo = p.d_m / 4.0f, q_hi = (float)l - q_lo;
+    const float sgn = ((l / 2) % 2 == 0) ? 1.0f : -1.0f;
+    std::vector<int> pairs;
+    for (int a = 0; a < na; ++a) {
+        bool any = false;
+        for (size_t i = (size_t)a * nwm * N; i < (size_t)(a + 1) * nwm * N && !any; ++i)
+            any = u[i].score >= thres && u[i].sigma > 0.0f;
+        if (!any) continue;
+        TRY(pair_spectra(ctx, angles[a], TS, false));
+        for (int wl = 0; wl < nwm; ++wl) {
+            const UnitOut* uw = u.data() + ((size_t)a * nwm + wl) * N;
+            pairs.clear();
+            for (int pp = 0; pp < Np; ++pp) {
+                bool sel = false;
+                for (int q = 0; q < 2 && 2 * pp + q < N; ++q)
+                    sel = sel || (uw[2 * pp + q].score >= thres && uw[2 * pp + q].sigma > 0.0f);
+                if (sel) pairs.push_back(pp);
+            }
+            if (pairs.empty()) continue;
+            const int w = mg.w0 + wl;
+            const float2* Ww = W + (long long)w * l2;
+            PixelMaxEpi epi;
+            epi.keys = keys;
+            epi.out = P<UnitOut>(ctx->units) + ((size_t)a * NW + w) * N;
+            epi.L = l;
+            epi.ntmpl = N;
+            epi.nx = mg.nx;
+            epi.offx = mg.offx[wl % bx];
+            epi.offy = mg.offy[wl / bx];
+            epi.idx0 = (unsigned int)a * (unsigned int)N;
+            epi.q_lo = q_lo;
+            epi.q_hi = q_hi;
+            epi.thres = thres;
+            epi.sgn = sgn;
+            for (size_t c0 = 0; c0 < pairs.size(); c0 += (size_t)chunk) {
+                const int nc = (int)std::min<size_t>((size_t)chunk, pairs.size() - c0);
+                // pageable source: the copy has completed when the call returns
+                CK(cudaMemcpyAsync(d_pairs, pairs.data() + c0, sizeof(int) * nc, cudaMemcpyHostToDevice, ctx->stream));
+                epi.pairs = d_pairs;
+                if (fast_ok(ctx, l)) {
+                    TRY(run_fast<true, false>(ctx, l, nc, F16Pass1Sel{Ww, TS, R, d_pairs, l, l2}));
+                    TRY(run_fast<true, true>(ctx, l, nc, F16Norm1<PixelMaxEpi>{R, epi, l, l2}));
+                } else {
+                    TRY(run_fft<true>(ctx, l, rows_of(l, l), nc, IoPass1Sel{Ww, TS, R, d_pairs, l2}));
+                    TRY(run_fft<true>(ctx, l, cols_of(l, l), nc, IoNorm1<PixelMaxEpi>{R, epi}));
+                }
+                CK(cudaStreamSynchronize(ctx->stream));  // d_pairs is rewritten by the next chunk
+            }
+        }
+    }
+    std::vector<unsigned long long> hk(npix);
+    CK(cudaMemcpyAsync(hk.data(), keys, sizeof(unsigned long long) * npix, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (size_t i = 0; i < npix; ++i) {
+        if (!hk[i]) {
+            value[i] = 0.0f;
+            if (tmpl) tmpl[i] = -1;
+            if (angle_out) angle_out[i] = -1;
+            continue;
+        }
+        value[i] = float_unorder((unsigned int)(hk[i] >> 32));
+        const unsigned int idx = ~(unsigned int)(hk[i] & 0xffffffffull);
+        if (tmpl) tmpl[i] = (int)(idx % (unsigned int)N);
+        if (angle_out) angle_out[i] = (int)(idx / (unsigned int)N);
+    }
     return GS_OK;
 }
 
@@ -1633,6 +1743,18 @@ int gs_get_units(gs_ctx* ctx, gs_unit* host_out, size_t cap, size_t* n_out) {
     CK(cudaSetDevice(ctx->device));
     CK(cudaMemcpy(host_out, ctx->units.p, sizeof(gs_unit) * total, cudaMemcpyDeviceToHost));
     return GS_OK;
+}
+
+int gs_get_pixel_max(gs_ctx* ctx, int micrograph, float thres, float* value, int* template_index,
+                     int* angle_index) {
+    if (!ctx || !value) return set_err(ctx, GS_ERR_ARG, "null pointer");
+    if (!std::isfinite(thres)) return set_err(ctx, GS_ERR_ARG, "threshold not finite");
+    if (!ctx->have_units)
+        return set_err(ctx, GS_ERR_STATE, "no norm_type 0 search has run (the map needs its units)");
+    if (micrograph < 0 || micrograph >= (int)ctx->last_mics.size())
+        return set_err(ctx, GS_ERR_ARG, "micrograph %d not in the last search", micrograph);
+    CK(cudaSetDevice(ctx->device));
+    return pixel_max_impl(ctx, micrograph, thres, value, template_index, angle_index);
 }
 
 void gs_picks_free(gs_pick* p) { free(p); }

@@ -182,6 +182,26 @@ int gs_search_device(struct gs_ctx* ctx, const float* device_micrograph, int nx,
  * Only a norm_type 0 search produces it (GS_ERR_STATE otherwise). */
 int gs_get_units(struct gs_ctx* ctx, gs_unit* host_out, size_t cap, size_t* n_out);
 
+/* Per-pixel maximum of the normalised correlation over (template, in-plane
+ * angle) for micrograph `micrograph` (0-based, in the order given) of the
+ * last norm_type 0 search.  No reference counterpart: the reference keeps
+ * one peak per (angle, window, template) map (main.cu:856-891), and the
+ * picks keep that rule; this map is an additional output.  Each map value
+ * is cc / sigma, sigma being that map's standard deviation without its peak
+ * as in the score (main.cu:869-876), so at a map's peak pixel it equals the
+ * unit's score.  Map pixel (X, Y) (fftshifted window index, as the picks'
+ * positions) lands on micrograph pixel (offx + X, offy + Y); the border the
+ * score's maximum leaves out (d_m / 4, GPU_func.cu:681) is left out here
+ * too, and overlapping windows merge by maximum.  Host outputs, nx * ny
+ * each, row-major: value (0 where no map reaches `thres`), template_index and
+ * angle_index (-1 there; either may be NULL).  Among equal values the
+ * smallest (angle, template) wins.  Only units whose score reaches `thres`
+ * are recomputed (no other unit can have a pixel at or above it), with the
+ * FP32 kernels whatever the search's precision; a low threshold costs up to
+ * a second search. */
+int gs_get_pixel_max(struct gs_ctx* ctx, int micrograph, float thres, float* value, int* template_index,
+                     int* angle_index);
+
 void gs_picks_free(gs_pick* picks);
 
 /* Timings of the last search, measured with CUDA events on the context's

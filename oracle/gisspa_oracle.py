@@ -589,19 +589,33 @@ class SearchResult:
     pos: np.ndarray = field(repr=False)
     peak: np.ndarray = field(repr=False)
     sd: np.ndarray = field(repr=False)
+    # per-pixel maximum of cc / sigma over (angle, template) (pixel_thres
+    # given): micrograph-sized value (NaN below the threshold) and the
+    # winning angle index and template (-1 below the threshold)
+    pixel_value: Optional[np.ndarray] = field(default=None, repr=False)
+    pixel_angle: Optional[np.ndarray] = field(default=None, repr=False)
+    pixel_template: Optional[np.ndarray] = field(default=None, repr=False)
 
 
 def search(micrograph: np.ndarray, templates_raw: np.ndarray, p: Params,
            ctf: Ctf, ctf_first: Optional[Ctf] = None, prepared: Optional[np.ndarray] = None,
            angles: Optional[Sequence[int]] = None, workers: int = 1,
-           dtype=np.complex128) -> SearchResult:
+           dtype=np.complex128, pixel_thres: Optional[float] = None) -> SearchResult:
     """One micrograph of the norm_type 0 search (main.cu:1149-1169, 1230-1257).
 
     ``templates_raw``: (N, ty, tx) float32 as read from the stack;
     ``ctf_first``: CTF of the first micrograph of the run (templates are
     weighted with it), defaults to ``ctf``; ``prepared``: precomputed output
     of :func:`prepare_templates`; ``angles``: optional subset of angle
-    indices (the dense tables then hold NaN elsewhere)."""
+    indices (the dense tables then hold NaN elsewhere).
+
+    ``pixel_thres`` (no reference counterpart): also build the per-pixel
+    maximum over (angle, template) of every map normalised by its own sigma
+    (the score's sigma, without the peak), over the non-border pixels the
+    score's maximum looks at, each map pixel placed at its particle centre
+    (window offset + fftshifted index) and the windows merged by maximum;
+    values below ``pixel_thres`` are left out.  Among equal values the first
+    in (angle, window, template) order wins."""
     ny, nx = micrograph.shape
     n, ty, tx = templates_raw.shape
     l = adjust_padding_size(p.padding_size, tx, ty)
@@ -622,6 +636,11 @@ def search(micrograph: np.ndarray, templates_raw: np.ndarray, p: Params,
     picks: List[Pick] = []
     d_m = float(f32(p.d_m))
     thres = f32(p.thres)
+    if pixel_thres is not None:
+        pix_v = np.full((ny, nx), -np.inf)
+        pix_a = np.full((ny, nx), -1, dtype=np.int64)
+        pix_t = np.full((ny, nx), -1, dtype=np.int64)
+        inner = ~border_mask(l, p.d_m)
     for ai in sel_angles:
         e = angs[ai]
         TS = template_spectra(T, e, p.d_m, workers).astype(dtype)
@@ -635,6 +654,16 @@ def search(micrograph: np.ndarray, templates_raw: np.ndarray, p: Params,
                 tab["peak"][ai, w] = st.peak
                 tab["sd"][ai, w] = st.sd
                 tab_pos[ai, w] = st.pos
+                if pixel_thres is not None:
+                    for J in range(n):
+                        if not (np.isfinite(st.score[J]) and st.sd[J] > 0):
+                            continue
+                        z = np.where(inner, cc[J] / st.sd[J], -np.inf)
+                        sub_v = pix_v[offy[j]:offy[j] + l, offx[i]:offx[i] + l]
+                        win = (z >= pixel_thres) & (z > sub_v)
+                        sub_v[win] = z[win]
+                        pix_a[offy[j]:offy[j] + l, offx[i]:offx[i] + l][win] = ai
+                        pix_t[offy[j]:offy[j] + l, offx[i]:offx[i] + l][win] = J
                 for J in range(n):
                     sc = st.score[J]
                     if not np.isfinite(sc) or f32(sc) < thres:
@@ -644,8 +673,12 @@ def search(micrograph: np.ndarray, templates_raw: np.ndarray, p: Params,
                     if cx >= d_m and cx < nx - d_m and cy >= d_m and cy < ny - d_m:
                         picks.append(Pick(ai, float(e), float(printed_phi(e)), i, j, J,
                                           cx, cy, float(sc)))
-    return SearchResult(picks, [float(a) for a in angs], offx, offy, l,
-                        tab["score"], tab_pos, tab["peak"], tab["sd"])
+    res = SearchResult(picks, [float(a) for a in angs], offx, offy, l,
+                       tab["score"], tab_pos, tab["peak"], tab["sd"])
+    if pixel_thres is not None:
+        res.pixel_value = np.where(np.isfinite(pix_v), pix_v, np.nan)
+        res.pixel_angle, res.pixel_template = pix_a, pix_t
+    return res
 
 
 @dataclass
