@@ -29,7 +29,7 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "out of memory", 3: "CUDA error",
           4: "invalid call order", 5: "unsupported input", 6: "device wait timed out",
           7: "I/O error"}
 # arithmetic of the correlation's DFT stages (gs_params.precision)
-GS_PREC_FP32, GS_PREC_TC_BF16, GS_PREC_TC_FP16 = 0, 1, 2
+GS_PREC_FP32, GS_PREC_TC_BF16, GS_PREC_TC_FP16, GS_PREC_TC_FULL, GS_PREC_TC_FULL_1P = 0, 1, 2, 3, 4
 
 
 class GsParams(C.Structure):

@@ -12,6 +12,7 @@
 #include "norm1.cuh"
 #include "pixmax.cuh"
 #include "tccorr.cuh"
+#include "tccorr2.cuh"
 #include "refine.cuh"
 
 #include <algorithm>
@@ -87,6 +88,7 @@ struct gs_ctx {
     int last_tuning[5] = {0, 0, 0, 0, 0};
     unsigned long long graph_kernel_launches = 0;
     DBuf unit_wp, dep_counters, pacc, flags;
+    DBuf tc2_wmax, tc2_pmax;  // per window / per pair max |spectrum| (all-tensor-core path)
     // off-grid refinement (refine.cuh): per-pick chunk buffers
     DBuf rf_pk, rf_acc, rf_B, rf_F1, rf_T, rf_TM, rf_F, rf_G, rf_TB, rf_mask;
     std::vector<cudaEvent_t> kev;  // pool of events for per-kernel timing
@@ -288,6 +290,25 @@ int launch_corr_tc_n2(gs_ctx* ctx, const CorrArgs& a, long long total_items) {
     // one CTA per SM: it runs C::kWg pipelines and holds the TMEM columns of
     // all of them (a second CTA would not fit in shared memory)
     const long long grid = std::min<long long>((long long)nsm, total_items);
+    kern<<<(unsigned)grid, C::kThreads, C::bytes, ctx->stream>>>(a);
+    ++ctx->counters.kernel_launches;
+    CKL();
+    return GS_OK;
+}
+
+// Persistent correlation with every DFT stage on the tensor cores (window
+// 720, tccorr2.cuh).  One CTA per SM: it allocates all 512 TMEM columns.
+template <int kProducts>
+int launch_corr_tc2_p(gs_ctx* ctx, const Tc2Args& a) {
+    using C = Tc2Cfg<kProducts>;
+    static_assert(2 * C::bytes > 228 * 1024, "a second CTA must not fit on an SM (TMEM is allocated whole)");
+    auto kern = k_corr_tc2<kProducts>;
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::bytes));
+    int nsm = 0, dev = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const long long total = (long long)(a.nu + a.lag) * 2 * C::T;
+    const long long grid = std::min<long long>((long long)nsm, total);
     kern<<<(unsigned)grid, C::kThreads, C::bytes, ctx->stream>>>(a);
     ++ctx->counters.kernel_launches;
     CKL();
@@ -852,7 +873,8 @@ static int validate_params(gs_ctx* ctx, const gs_params* p) {
         return set_err(ctx, GS_ERR_ARG, "required parameter missing or not positive");
     if (p->norm_type != 0 && p->norm_type != 1)
         return set_err(ctx, GS_ERR_ARG, "norm_type must be 0 or 1 (got %d)", p->norm_type);
-    if (p->precision != GS_PREC_FP32 && p->precision != GS_PREC_TC_BF16 && p->precision != GS_PREC_TC_FP16)
+    if (p->precision != GS_PREC_FP32 && p->precision != GS_PREC_TC_BF16 && p->precision != GS_PREC_TC_FP16 &&
+        p->precision != GS_PREC_TC_FULL && p->precision != GS_PREC_TC_FULL_1P)
         return set_err(ctx, GS_ERR_ARG, "unknown precision mode %d", p->precision);
     if (p->precision != GS_PREC_FP32 && p->norm_type != 0)
         return set_err(ctx, GS_ERR_UNSUPPORTED, "tensor-core precision modes need norm_type 0");
@@ -1145,6 +1167,19 @@ static int corr_launch(gs_ctx* ctx, const float2* W, const float2* TS, int nu, c
     }
     ctx->corr_ctas_override = t.ctas;
     if (ctx->p.precision == GS_PREC_FP32) return launch_corr(ctx, l, t.tile, ca);
+    if (ctx->p.precision == GS_PREC_TC_FULL || ctx->p.precision == GS_PREC_TC_FULL_1P) {
+        if (l != 720) return set_err(ctx, GS_ERR_UNSUPPORTED, "the all-tensor-core path takes window 720 (got %d)", l);
+        Tc2Args a;
+        a.W = ca.W; a.P = ca.P;
+        a.R = P<__half2>(ctx->scratch);
+        a.wmax = P<float>(ctx->tc2_wmax);
+        a.pmax = P<float>(ctx->tc2_pmax);
+        a.unit_wp = ca.unit_wp; a.done_rows = ca.done_rows; a.done_cols = ca.done_cols;
+        a.acc = ca.acc; a.out = ca.out; a.next_item = ca.next_item; a.error = ca.error;
+        a.nu = ca.nu; a.ntmpl = ca.ntmpl; a.S = ca.S; a.lag = ca.lag; a.L2 = ca.L2;
+        a.yb0 = ca.yb0; a.yb1 = ca.yb1;
+        return ctx->p.precision == GS_PREC_TC_FULL ? launch_corr_tc2_p<2>(ctx, a) : launch_corr_tc2_p<1>(ctx, a);
+    }
     return launch_corr_tc(ctx, l, ctx->p.precision == GS_PREC_TC_BF16, ca);
 }
 
@@ -1234,7 +1269,10 @@ static int correlate_all(gs_ctx* ctx, float2* W, int NW, const std::vector<float
     const bool persistent = fast_ok(ctx, l) && !ctx->two_pass;
     // the FP32 persistent kernel at window 720 takes prime-factor transforms
     // and reads its spectra in PfaCols column order
-    const bool pfa = persistent && p.precision == GS_PREC_FP32 && PfaCols::make(l).N2 != 0;
+    const bool tc2 = p.precision == GS_PREC_TC_FULL || p.precision == GS_PREC_TC_FULL_1P;
+    if (tc2 && l != 720)
+        return set_err(ctx, GS_ERR_UNSUPPORTED, "the all-tensor-core path takes window 720 (got %d)", l);
+    const bool pfa = persistent && (p.precision == GS_PREC_FP32 || tc2) && PfaCols::make(l).N2 != 0;
     if (p.precision != GS_PREC_FP32 && !persistent)
         return set_err(ctx, GS_ERR_UNSUPPORTED,
                        "tensor-core precision needs window 512, 720 or 768 and the persistent path (window %d)", l);
@@ -1272,6 +1310,15 @@ static int correlate_all(gs_ctx* ctx, float2* W, int NW, const std::vector<float
         }
     } pfa_w{ctx, W, (long long)NW * l, PfaCols::make(l)};
     if (pfa) TRY(pfa_w.set(true));
+    if (tc2) {
+        // per-window max |W| for the FP16 scaling of each unit
+        TRY(ensure(ctx, ctx->tc2_wmax, sizeof(float) * NW));
+        TRY(ensure(ctx, ctx->tc2_pmax, sizeof(float) * Np));
+        CK(cudaMemsetAsync(ctx->tc2_wmax.p, 0, sizeof(float) * NW, ctx->stream));
+        k_max_abs<<<dim3(64, NW), 256, 0, ctx->stream>>>(W, l2, P<float>(ctx->tc2_wmax));
+        ++ctx->counters.kernel_launches;
+        CKL();
+    }
     if (persistent) {
         TRY(ensure(ctx, ctx->dep_counters, sizeof(int) * (2 * (size_t)nu + 4)));
         TRY(ensure(ctx, ctx->pacc, sizeof(UnitAcc) * 2 * (size_t)nu));
@@ -1280,6 +1327,12 @@ static int correlate_all(gs_ctx* ctx, float2* W, int NW, const std::vector<float
         if (ctx->autotune) {
             TRY(ensure(ctx, ctx->scratch, sizeof(float2) * l2 * 32));
             TRY(pair_spectra(ctx, angles[0], TS, pfa));
+            if (tc2) {
+                CK(cudaMemsetAsync(ctx->tc2_pmax.p, 0, sizeof(float) * Np, ctx->stream));
+                k_max_abs<<<dim3(64, Np), 256, 0, ctx->stream>>>(TS, l2, P<float>(ctx->tc2_pmax));
+                ++ctx->counters.kernel_launches;
+                CKL();
+            }
             TRY(autotune(ctx, W, TS, NW, &tune));
         }
         TRY(upload_unit_order(ctx, NW, Np, tune.window_block, nu));
@@ -1317,6 +1370,12 @@ static int correlate_all(gs_ctx* ctx, float2* W, int NW, const std::vector<float
     auto enqueue_angle = [&](int ai, bool rec) -> int {
         if (rec) CK(cudaEventRecord(ea, ctx->stream));
         TRY(pair_spectra(ctx, angles[ai], TS, pfa));
+        if (tc2) {
+            CK(cudaMemsetAsync(ctx->tc2_pmax.p, 0, sizeof(float) * Np, ctx->stream));
+            k_max_abs<<<dim3(64, Np), 256, 0, ctx->stream>>>(TS, l2, P<float>(ctx->tc2_pmax));
+            ++ctx->counters.kernel_launches;
+            CKL();
+        }
         if (rec) CK(cudaEventRecord(eb, ctx->stream));
         if (persistent) {
             if (timing) CK(cudaEventRecord(ctx->kev[0], ctx->stream));

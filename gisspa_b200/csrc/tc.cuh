@@ -27,6 +27,15 @@ __host__ __device__ __forceinline__ uint32_t kmajor_off(int r, int k, int R) {
     return (uint32_t)((k >> 3) * (R >> 3) * 128 + (r >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
 }
 
+// Byte offset of element (mn, k) in an MN-major, no-swizzle operand: core
+// matrices of 8 K-rows x 16 bytes (8 sixteen-bit MN elements), the 8-element
+// MN groups `sbo` bytes apart and the 8-row K groups `lbo` bytes apart (the
+// descriptor's stride and leading byte offsets for this major-ness).  The
+// MMA over K elements [16 j, 16 j + 16) starts at byte 2 j lbo.
+__host__ __device__ __forceinline__ uint32_t mnmajor_off(int mn, int k, uint32_t sbo, uint32_t lbo) {
+    return (uint32_t)((mn >> 3) * sbo + (k >> 3) * lbo + (k & 7) * 16 + (mn & 7) * 2);
+}
+
 // Shared-memory matrix descriptor: start address, leading (K-chunk) and
 // stride (8-row group) byte offsets, descriptor version 1, no swizzle.
 __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
@@ -46,6 +55,10 @@ __host__ __device__ constexpr uint32_t idesc_f16(int M, int N, int ab_bf16) {
            | ((uint32_t)ab_bf16 << 10)        // B format
            | ((uint32_t)(N >> 3) << 17)       // N / 8
            | ((uint32_t)(M >> 4) << 24);      // M / 16
+}
+// The same with A and / or B MN-major (bits 15 and 16).
+__host__ __device__ constexpr uint32_t idesc_f16_major(int M, int N, int ab_bf16, int a_mn, int b_mn) {
+    return idesc_f16(M, N, ab_bf16) | ((uint32_t)a_mn << 15) | ((uint32_t)b_mn << 16);
 }
 
 // ---- mbarrier ----

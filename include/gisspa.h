@@ -77,6 +77,17 @@ typedef struct gs_params {
 #define GS_PREC_FP32 0
 #define GS_PREC_TC_BF16 1
 #define GS_PREC_TC_FP16 2
+/* GS_PREC_TC_FULL / GS_PREC_TC_FULL_1P (window 720, persistent path,
+ * norm_type 0): every DFT stage of the correlation (16- and 45-point, both
+ * passes) runs on the tensor cores with FP16 operands and FP32 accumulation,
+ * the data rounded to FP16 once per stage and the DFT matrix split into
+ * (hi, lo) FP16 parts (two products) or rounded once (_1P, one product); each
+ * unit's spectrum is scaled by a power of two to stay inside the FP16 range
+ * and the row-pass maps are kept in FP16.  Scores stay within 1e-3 relative
+ * of the FP64 oracle (a few 1e-4 measured); other windows return
+ * GS_ERR_UNSUPPORTED. */
+#define GS_PREC_TC_FULL 3
+#define GS_PREC_TC_FULL_1P 4
 
 /* Per-micrograph CTF line values as in the input list
  * (DataReader.cpp:366-388: defocus=, dfdiff=, dfang=). */
