@@ -161,7 +161,7 @@ __device__ __forceinline__ void tc2_sync(int g) { asm volatile("bar.sync %0, 128
 // Issue a GEMM stage (thread 0 of the pipeline), commit, wait for it (one
 // lane per warp polls the mbarrier).  Returns false when the bounded wait gave up.
 template <class C, bool kStage2, bool kColPass>
-__device__ __forceinline__ bool tc2_gemm(const Tc2Wg& w, unsigned char* sm, uint32_t& phase) {
+__device__ __forceinline__ bool tc2_gemm(const Tc2Wg& w, unsigned char* sm, uint32_t& phase, const int* a_error) {
     tc::fence_async_smem();
     tc::fence_before_sync();
     tc2_sync(w.g);
@@ -197,7 +197,10 @@ __device__ __forceinline__ bool tc2_gemm(const Tc2Wg& w, unsigned char* sm, uint
     }
     __syncwarp();
     int ok = 1;
-    if ((threadIdx.x & 31) == 0) ok = tc::mbar_wait(w.bar, phase, 1u << 24) ? 1 : 0;
+    // once any wait of the launch has given up, later waits end quickly
+    if ((threadIdx.x & 31) == 0)
+        ok = tc::mbar_wait(w.bar, phase, *(volatile int*)a_error ? (1u << 12) : (1u << 24)) ? 1 : 0;
+    if (!ok && (threadIdx.x & 31) == 0) atomicExch(const_cast<int*>(a_error), 1);
     ok = __shfl_sync(0xffffffffu, ok, 0);
     phase ^= 1u;
     tc::fence_after_sync();
@@ -415,12 +418,15 @@ __device__ __forceinline__ void tc2_finish_unit(const Tc2Args& a, int u) {
     }
 }
 
+// Bounded (about a second); gives up at once when another wait of the
+// launch has already given up (error flag set), so a failed launch ends soon.
 template <class C>
 __device__ __forceinline__ void tc2_wait_counter(const int* p, int target, int* error) {
     if (ld_acquire_gpu(p) >= target) return;
     for (int it = 0; it < (1 << 22); ++it) {
         __nanosleep(256);
         if (ld_acquire_gpu(p) >= target) return;
+        if ((it & 1023) == 1023 && *(volatile int*)error) return;
     }
     atomicExch(error, 1);
 }
@@ -482,9 +488,9 @@ __global__ void __launch_bounds__(Tc2Cfg<kProducts>::kThreads, 1) k_corr_tc2(Tc2
                 const int2 wp = __ldg(a.unit_wp + s);
                 const float sc = tc2_scale(__ldg(a.wmax + wp.x), __ldg(a.pmax + wp.y));
                 tc2_row_fill<C>(a, s, j, w, sc);
-                ok &= tc2_gemm<C, false, false>(w, sm, phase);
+                ok &= tc2_gemm<C, false, false>(w, sm, phase, a.error);
                 tc2_transition<C>(w);
-                ok &= tc2_gemm<C, true, false>(w, sm, phase);
+                ok &= tc2_gemm<C, true, false>(w, sm, phase, a.error);
                 tc2_row_out<C>(a, s, j, w);
                 __syncwarp();
                 if ((threadIdx.x & 31) == 0)
@@ -494,9 +500,9 @@ __global__ void __launch_bounds__(Tc2Cfg<kProducts>::kThreads, 1) k_corr_tc2(Tc2
             const int u = s - a.lag;
             if (u >= 0 && u < a.nu) {
                 tc2_col_fill<C>(a, u, j - C::T, w);
-                ok &= tc2_gemm<C, false, true>(w, sm, phase);
+                ok &= tc2_gemm<C, false, true>(w, sm, phase, a.error);
                 tc2_transition<C>(w);
-                ok &= tc2_gemm<C, true, true>(w, sm, phase);
+                ok &= tc2_gemm<C, true, true>(w, sm, phase, a.error);
                 tc2_col_out<C>(a, u, j - C::T, w);
                 __syncwarp();
                 if ((threadIdx.x & 31) == 0) {
