@@ -242,16 +242,34 @@ __device__ __forceinline__ void tc2_row_fill(const Tc2Args& a, int u, int t, con
     const unsigned long long keep = l2_policy_evict_last();
     const int warp = w.wt >> 5, lane = w.wt & 31;
     // every warp takes 32-column chunks of the tile's rows: 23 chunks per row
-    // (the last one 16 wide), 184 per tile
-    for (int q = warp; q < C::V * 23; q += 4) {
-        const int v = q / 23, c = (q - v * 23) * 32 + lane;
-        if (c >= C::L) continue;
-        const int n1 = c / C::N2, n2 = c - n1 * C::N2;
-        const long long o = (long long)C::Pfa::spectrum_row(8 * t + v) * C::L + c;
-        const float2 x = cmulc(ld_l2hint(Wr + o, keep), __ldg(Pr + o));
-        const int m = v + 8 * n1;
-        *reinterpret_cast<uint32_t*>(w.a + (uint32_t)(n2 >> 2) * C::LBO1R + (uint32_t)(m >> 3) * 128 +
-                                     (uint32_t)(m & 7) * 16 + (uint32_t)(n2 & 3) * 4) = pack_half2(x.x * s, x.y * s);
+    // (the last one 16 wide), 184 per tile, chunk q = 4 i + warp; kB chunks
+    // are loaded before any is used so that their L2 round trips overlap
+    constexpr int kChunks = C::V * 23, kB = 8;
+    for (int q0 = warp; q0 < kChunks; q0 += 4 * kB) {
+        float2 wv[kB], pv[kB];
+#pragma unroll
+        for (int b = 0; b < kB; ++b) {
+            const int q = q0 + 4 * b;
+            const int v = q / 23, c = (q - v * 23) * 32 + lane;
+            if (q < kChunks && c < C::L) {
+                const long long o = (long long)C::Pfa::spectrum_row(8 * t + v) * C::L + c;
+                wv[b] = ld_l2hint(Wr + o, keep);
+                pv[b] = __ldg(Pr + o);
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < kB; ++b) {
+            const int q = q0 + 4 * b;
+            const int v = q / 23, c = (q - v * 23) * 32 + lane;
+            if (q < kChunks && c < C::L) {
+                const int n1 = c / C::N2, n2 = c - n1 * C::N2;
+                const float2 x = cmulc(wv[b], pv[b]);
+                const int m = v + 8 * n1;
+                *reinterpret_cast<uint32_t*>(w.a + (uint32_t)(n2 >> 2) * C::LBO1R + (uint32_t)(m >> 3) * 128 +
+                                             (uint32_t)(m & 7) * 16 + (uint32_t)(n2 & 3) * 4) =
+                    pack_half2(x.x * s, x.y * s);
+            }
+        }
     }
     // K padding n2 = 45 .. 47 (K group 11, entries 1 .. 3): zero (their B rows are zero too)
     for (int i = w.wt; i < 128 * 3; i += 128) {
