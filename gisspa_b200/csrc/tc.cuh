@@ -86,6 +86,34 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32
     return false;
 }
 
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Waits until the barrier's phase with the given parity has completed,
+// suspending the thread inside try_wait (up to `hint_ns` per attempt, woken
+// when the phase completes) instead of spinning, so a waiting warp takes no
+// issue slots; gives up after `limit_ns` of wall time (returns false).
+__device__ __forceinline__ bool mbar_wait_suspend(uint64_t* bar, uint32_t parity, uint32_t hint_ns,
+                                                  uint64_t limit_ns) {
+    const uint32_t a = smem_u32(bar);
+    const uint64_t t0 = globaltimer_ns();
+    for (;;) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity), "r"(hint_ns)
+            : "memory");
+        if (done) return true;
+        if (globaltimer_ns() - t0 > limit_ns) return false;
+    }
+}
+
 // ---- fences ----
 // st.shared writes -> visible to the tensor core's (async proxy) reads
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }

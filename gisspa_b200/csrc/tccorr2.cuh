@@ -183,12 +183,14 @@ __device__ __forceinline__ bool tc2_gemm(const Tc2Wg& w, unsigned char* sm, uint
         } else {
             const uint32_t b = tc::smem_u32(sm + C::off_b16);
             constexpr uint32_t lbo_b = C::K2 * 16;
+            // the three M-tiles' accumulators are independent: interleave
+            // them so that consecutive MMAs do not wait on one another
 #pragma unroll
-            for (int t = 0; t < C::MT2; ++t)
+            for (int j = 0; j < C::K2 / 16; ++j)
 #pragma unroll
-                for (int j = 0; j < C::K2 / 16; ++j)
+                for (int p = 0; p < C::kProducts; ++p)
 #pragma unroll
-                    for (int p = 0; p < C::kProducts; ++p)
+                    for (int t = 0; t < C::MT2; ++t)
                         tc::mma_f16(w.tmem + 32 * t, tc::smem_desc(a + t * 2048 + 2 * j * C::LBO2, C::LBO2, 128),
                                     tc::smem_desc(b + p * C::b16_bytes + 2 * j * lbo_b, lbo_b, 128), C::idesc2,
                                     (j | p) ? 1u : 0u);
@@ -198,8 +200,11 @@ __device__ __forceinline__ bool tc2_gemm(const Tc2Wg& w, unsigned char* sm, uint
     __syncwarp();
     int ok = 1;
     // once any wait of the launch has given up, later waits end quickly
+    // lane 0 sleeps in try_wait until the MMAs complete (bounded: 2 s, or
+    // 1 ms once any wait of the launch has given up)
     if ((threadIdx.x & 31) == 0)
-        ok = tc::mbar_wait(w.bar, phase, *(volatile int*)a_error ? (1u << 12) : (1u << 24)) ? 1 : 0;
+        ok = tc::mbar_wait_suspend(w.bar, phase, 100000u,
+                                   *(volatile int*)a_error ? 1000000ull : 2000000000ull) ? 1 : 0;
     if (!ok && (threadIdx.x & 31) == 0) atomicExch(const_cast<int*>(a_error), 1);
     ok = __shfl_sync(0xffffffffu, ok, 0);
     phase ^= 1u;
@@ -241,34 +246,29 @@ __device__ __forceinline__ void tc2_row_fill(const Tc2Args& a, int u, int t, con
     const float2* Pr = a.P + (long long)wp.y * a.L2;
     const unsigned long long keep = l2_policy_evict_last();
     const int warp = w.wt >> 5, lane = w.wt & 31;
-    // every warp takes 32-column chunks of the tile's rows: 23 chunks per row
-    // (the last one 16 wide), 184 per tile, chunk q = 4 i + warp; kB chunks
-    // are loaded before any is used so that their L2 round trips overlap
-    constexpr int kChunks = C::V * 23, kB = 8;
-    for (int q0 = warp; q0 < kChunks; q0 += 4 * kB) {
-        float2 wv[kB], pv[kB];
+    // 32-column chunks: warp w takes chunks j = w, w + 4, ... (23 per row, the
+    // last 16 wide) of all 8 rows, so a lane's column, its prime-factor
+    // indices and its shared-memory offset serve 8 values, and the 16 loads
+    // of a chunk are in flight together
+    long long srow[C::V];
 #pragma unroll
-        for (int b = 0; b < kB; ++b) {
-            const int q = q0 + 4 * b;
-            const int v = q / 23, c = (q - v * 23) * 32 + lane;
-            if (q < kChunks && c < C::L) {
-                const long long o = (long long)C::Pfa::spectrum_row(8 * t + v) * C::L + c;
-                wv[b] = ld_l2hint(Wr + o, keep);
-                pv[b] = __ldg(Pr + o);
-            }
+    for (int v = 0; v < C::V; ++v) srow[v] = (long long)C::Pfa::spectrum_row(8 * t + v) * C::L;
+    for (int j = warp; j < 23; j += 4) {
+        const int c = 32 * j + lane;
+        if (c >= C::L) continue;
+        const int n1 = c / C::N2, n2 = c - n1 * C::N2;
+        unsigned char* dst = w.a + (uint32_t)(n2 >> 2) * C::LBO1R + (uint32_t)n1 * 128 + (uint32_t)(n2 & 3) * 4;
+        float2 wv[C::V], pv[C::V];
+#pragma unroll
+        for (int v = 0; v < C::V; ++v) {
+            wv[v] = ld_l2hint(Wr + srow[v] + c, keep);
+            pv[v] = __ldg(Pr + srow[v] + c);
         }
 #pragma unroll
-        for (int b = 0; b < kB; ++b) {
-            const int q = q0 + 4 * b;
-            const int v = q / 23, c = (q - v * 23) * 32 + lane;
-            if (q < kChunks && c < C::L) {
-                const int n1 = c / C::N2, n2 = c - n1 * C::N2;
-                const float2 x = cmulc(wv[b], pv[b]);
-                const int m = v + 8 * n1;
-                *reinterpret_cast<uint32_t*>(w.a + (uint32_t)(n2 >> 2) * C::LBO1R + (uint32_t)(m >> 3) * 128 +
-                                             (uint32_t)(m & 7) * 16 + (uint32_t)(n2 & 3) * 4) =
-                    pack_half2(x.x * s, x.y * s);
-            }
+        for (int v = 0; v < C::V; ++v) {
+            const float2 x = cmulc(wv[v], pv[v]);
+            // row m = v + 8 n1 of the operand: 8-row group n1, row v in it
+            *reinterpret_cast<uint32_t*>(dst + (uint32_t)v * 16) = pack_half2(x.x * s, x.y * s);
         }
     }
     // K padding n2 = 45 .. 47 (K group 11, entries 1 .. 3): zero (their B rows are zero too)
@@ -372,10 +372,13 @@ __device__ __forceinline__ void tc2_col_out(const Tc2Args& a, int u, int t, cons
         tc::tmem_ld_wait();
         const int k2 = 16 * ti + (w.wt >> 3);
         if (k2 >= C::N2) continue;
+        const int ybase = (C::Pfa::A2 * k2) % L;
 #pragma unroll
         for (int k1 = 0; k1 < 16; ++k1) {
             const float v1 = __uint_as_float(r[2 * k1]), v2 = __uint_as_float(r[2 * k1 + 1]);
-            const int y = C::Pfa::map_coord(k1, k2);
+            // map row (A1 k1 + A2 k2) mod L, the k1 part a compile-time constant
+            int y = ybase + (C::Pfa::A1 * k1) % L;
+            y -= y >= L ? L : 0;
             const bool in = !xin && ((unsigned)(y - a.yb0) > (unsigned)(a.yb1 - a.yb0));
             const bool g1 = in && v1 > best1, g2 = in && v2 > best2;
             best1 = g1 ? v1 : best1;
