@@ -69,7 +69,7 @@ struct Tc2Cfg {
     static constexpr int M2 = V * N2P;          // stage-2 rows (k2, v), 384
     static constexpr int MT2 = M2 / 128;        // stage-2 M-tiles
     static constexpr int K2 = 32;               // stage 2: K = N = 2 x 16
-    static constexpr int kWg = 4;               // pipelines per CTA
+    static constexpr int kWg = 5;               // pipelines per CTA
     static constexpr int kThreads = 128 * kWg;
     static constexpr int kDone = 4 * T;         // warp completions per pass of a unit
     // stage-1 operand, row pass: K-major, 8-row groups 128 B apart, 8-element
@@ -90,7 +90,7 @@ struct Tc2Cfg {
     static constexpr size_t off_bar = off_a + (size_t)kWg * a_bytes;
     static constexpr size_t off_misc = off_bar + 8 * kWg;  // tmem slot (16 B), then 4 claim slots per pipeline
     static constexpr size_t bytes = off_misc + 16 + (size_t)16 * kWg;
-    static constexpr uint32_t tmem_cols = 128;            // per pipeline (96 used)
+    static constexpr uint32_t tmem_cols = 96;             // per pipeline (stage 1 N = 96; stage 2 3 x 32, aliased)
     static constexpr uint32_t idesc1r = tc::idesc_f16_major(128, K1, 0, 0, 0);
     static constexpr uint32_t idesc1c = tc::idesc_f16_major(128, K1, 0, 1, 0);
     static constexpr uint32_t idesc2 = tc::idesc_f16_major(128, K2, 0, 0, 0);
@@ -220,16 +220,13 @@ __device__ __forceinline__ void tc2_transition(const Tc2Wg& w) {
     const uint32_t lane_base = w.tmem + ((uint32_t)(32 * (w.wt >> 5)) << 16);
     uint32_t r[32];
     unsigned char* dst = w.a + (uint32_t)(n1 >> 2) * C::LBO2 + (uint32_t)v * 16 + (uint32_t)(n1 & 3) * 4;
-#pragma unroll
+#pragma unroll 1
     for (int q = 0; q < 3; ++q) {
         tc::tmem_ld32(lane_base + 32 * q, r);
         tc::tmem_ld_wait();
-        if (q == 0) {
-            // all 128 lanes of D1 are being read: A1 (aliased by A2) is no
-            // longer needed by the finished MMA, so the stores below may start
-        }
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
+            // A1 (aliased by A2) is no longer read: the stage-1 MMAs completed
             const int k2 = 16 * q + i;
             *reinterpret_cast<uint32_t*>(dst + (uint32_t)k2 * 128) =
                 pack_half2(__uint_as_float(r[2 * i]), __uint_as_float(r[2 * i + 1]));
@@ -250,9 +247,9 @@ __device__ __forceinline__ void tc2_row_fill(const Tc2Args& a, int u, int t, con
     // last 16 wide) of all 8 rows, so a lane's column, its prime-factor
     // indices and its shared-memory offset serve 8 values, and the 16 loads
     // of a chunk are in flight together
-    long long srow[C::V];
+    int srow[C::V];
 #pragma unroll
-    for (int v = 0; v < C::V; ++v) srow[v] = (long long)C::Pfa::spectrum_row(8 * t + v) * C::L;
+    for (int v = 0; v < C::V; ++v) srow[v] = C::Pfa::spectrum_row(8 * t + v) * C::L;
     for (int j = warp; j < 23; j += 4) {
         const int c = 32 * j + lane;
         if (c >= C::L) continue;
@@ -287,11 +284,13 @@ __device__ __forceinline__ void tc2_col_fill(const Tc2Args& a, int u, int t, con
     const __half2* Rs = a.R + (long long)(u % a.S) * a.L2;
     const unsigned long long drop = l2_policy_evict_first();
     constexpr int kChunks = 2 * C::L;  // (row, half)
-    constexpr int kPer = (kChunks + 127) / 128;
+    constexpr int kPer = 6;            // 16-byte chunks in flight per thread
+    static_assert(kChunks <= 2 * kPer * 128, "two batches");
+    for (int base = 0; base < kChunks; base += kPer * 128) {
     uint4 vals[kPer];
 #pragma unroll
     for (int i = 0; i < kPer; ++i) {
-        const int q = w.wt + 128 * i;
+        const int q = base + w.wt + 128 * i;
         if (q < kChunks) {
             const int r = q >> 1, h = q & 1;
             const uint4* src = reinterpret_cast<const uint4*>(Rs + (long long)r * C::L + 8 * t) + h;
@@ -302,12 +301,13 @@ __device__ __forceinline__ void tc2_col_fill(const Tc2Args& a, int u, int t, con
     }
 #pragma unroll
     for (int i = 0; i < kPer; ++i) {
-        const int q = w.wt + 128 * i;
+        const int q = base + w.wt + 128 * i;
         if (q < kChunks) {
             const int r = q >> 1, h = q & 1;
             const int n1 = r / C::N2, n2 = r - n1 * C::N2;
             *reinterpret_cast<uint4*>(w.a + (uint32_t)n1 * C::SBO1C + (uint32_t)n2 * 32 + (uint32_t)h * 16) = vals[i];
         }
+    }
     }
     // K padding rows n2 = 45 .. 47 of every n1 group: zero
     for (int i = w.wt; i < 16 * 3 * 2; i += 128) {
@@ -325,7 +325,7 @@ __device__ __forceinline__ void tc2_row_out(const Tc2Args& a, int u, int t, cons
     const uint32_t lane_base = w.tmem + ((uint32_t)(32 * (w.wt >> 5)) << 16);
     const int v = w.wt & 7;
     const unsigned long long keep = l2_policy_evict_last();
-#pragma unroll
+#pragma unroll 1
     for (int ti = 0; ti < C::MT2; ++ti) {
         uint32_t r[32];
         tc::tmem_ld32(lane_base + 32 * ti, r);
@@ -351,55 +351,96 @@ __device__ __forceinline__ void tc2_row_out(const Tc2Args& a, int u, int t, cons
     }
 }
 
-// Column-pass epilogue: values of map column x (physical column 8 t + v),
-// rows map_coord(k1, k2): border-masked peak with its position and the sum
-// of squares, both templates, reduced per warp into the unit's accumulators.
+// Border mask of the map rows this thread's stage-2 lanes hold: bit k1 of
+// word ti is set when map row (A1 k1 + A2 k2) mod L, k2 = 16 ti + wt / 8, lies
+// inside the maximum's interior (outside the border interval [yb0, yb1]).
+// Fixed for the life of the kernel.
+struct Tc2Masks {
+    uint32_t m[3];
+};
 template <class C>
-__device__ __forceinline__ void tc2_col_out(const Tc2Args& a, int u, int t, const Tc2Wg& w) {
-    constexpr int L = C::L, h = L / 2;
-    const uint32_t lane_base = w.tmem + ((uint32_t)(32 * (w.wt >> 5)) << 16);
-    const int v = w.wt & 7;
-    const int pc = 8 * t + v;                                   // physical column
-    const int x = C::Pfa::map_coord(pc & 15, pc >> 4);           // map column
-    const bool xin = (unsigned)(x - a.yb0) <= (unsigned)(a.yb1 - a.yb0);
-    float best1 = 0.0f, best2 = 0.0f;
-    int by1 = -1, by2 = -1;
-    float s2a = 0.0f, s2b = 0.0f;
+__device__ __forceinline__ Tc2Masks tc2_row_masks(int wt, int yb0, int yb1) {
+    Tc2Masks mk;
 #pragma unroll
+    for (int ti = 0; ti < C::MT2; ++ti) {
+        const int k2 = 16 * ti + (wt >> 3);
+        uint32_t m = 0u;
+        if (k2 < C::N2)
+            for (int k1 = 0; k1 < 16; ++k1) {
+                const int y = C::Pfa::map_coord(k1, k2);
+                if ((unsigned)(y - yb0) > (unsigned)(yb1 - yb0)) m |= 1u << k1;
+            }
+        mk.m[ti] = m;
+    }
+    return mk;
+}
+
+// Column-pass epilogue: values of map column x (physical column 8 t + v),
+// rows map_coord(k1, k2), both templates of the pair: the sum of squares and
+// the border-masked maximum (starting at 0, as the reference's peak) per
+// thread, the maximum reduced over the warp, and only the lanes holding the
+// warp's maximum look for its position (re-reading their TMEM lanes); the
+// warp then adds its share to the unit's accumulators.
+template <class C>
+__device__ __forceinline__ void tc2_col_out(const Tc2Args& a, int u, int t, const Tc2Wg& w, const Tc2Masks mb) {
+    constexpr int L = C::L, h = L / 2;
+    static_assert((L / 2) % 2 == 0, "sign of the fftshift: (-1)^(L/2) = +1");
+    const uint32_t lane_base = w.tmem + ((uint32_t)(32 * (w.wt >> 5)) << 16);
+    const int pc = 8 * t + (w.wt & 7);                           // physical column
+    const int x = C::Pfa::map_coord(pc & 15, pc >> 4);           // map column
+    const bool xin = (unsigned)(x - a.yb0) <= (unsigned)(a.yb1 - a.yb0);  // column in the border
+    float m1 = 0.0f, m2 = 0.0f, s2a = 0.0f, s2b = 0.0f;
+    // the tile loops stay rolled: one 32-register array is live at a time
+#pragma unroll 1
     for (int ti = 0; ti < C::MT2; ++ti) {
         uint32_t r[32];
         tc::tmem_ld32(lane_base + 32 * ti, r);
         tc::tmem_ld_wait();
-        const int k2 = 16 * ti + (w.wt >> 3);
-        if (k2 >= C::N2) continue;
-        const int ybase = (C::Pfa::A2 * k2) % L;
+        // rows k2 >= 45 hold zeros and no bits
+        const uint32_t bits = xin ? 0u : (ti == 0 ? mb.m[0] : ti == 1 ? mb.m[1] : mb.m[2]);
 #pragma unroll
         for (int k1 = 0; k1 < 16; ++k1) {
             const float v1 = __uint_as_float(r[2 * k1]), v2 = __uint_as_float(r[2 * k1 + 1]);
-            // map row (A1 k1 + A2 k2) mod L, the k1 part a compile-time constant
-            int y = ybase + (C::Pfa::A1 * k1) % L;
-            y -= y >= L ? L : 0;
-            const bool in = !xin && ((unsigned)(y - a.yb0) > (unsigned)(a.yb1 - a.yb0));
-            const bool g1 = in && v1 > best1, g2 = in && v2 > best2;
-            best1 = g1 ? v1 : best1;
-            by1 = g1 ? y : by1;
-            best2 = g2 ? v2 : best2;
-            by2 = g2 ? y : by2;
+            const bool in = (bits >> k1) & 1u;
+            m1 = fmaxf(m1, in ? v1 : 0.0f);
+            m2 = fmaxf(m2, in ? v2 : 0.0f);
             s2a = fmaf(v1, v1, s2a);
             s2b = fmaf(v2, v2, s2b);
         }
     }
-    // sign of the fftshift: (-1)^(L/2) = +1 at L = 720
-    static_assert((L / 2) % 2 == 0, "sign");
-    const int X = x + h < L ? x + h : x - h;
-    unsigned long long ka = 0ull, kb = 0ull;
-    if (by1 >= 0) {
-        const int Y = by1 + h < L ? by1 + h : by1 - h;
-        ka = argmax_key(best1, Y * L + X);
+    float M1 = m1, M2 = m2;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        M1 = fmaxf(M1, __shfl_xor_sync(0xffffffffu, M1, o));
+        M2 = fmaxf(M2, __shfl_xor_sync(0xffffffffu, M2, o));
     }
-    if (by2 >= 0) {
-        const int Y = by2 + h < L ? by2 + h : by2 - h;
-        kb = argmax_key(best2, Y * L + X);
+    unsigned long long ka = 0ull, kb = 0ull;
+    if (M1 > 0.0f || M2 > 0.0f) {   // warp-uniform: every lane re-reads its TMEM lanes
+        const bool look1 = M1 > 0.0f && m1 == M1, look2 = M2 > 0.0f && m2 == M2;
+        const int X = x + h < L ? x + h : x - h;
+        int i1 = 0x7fffffff, i2 = 0x7fffffff;
+#pragma unroll 1
+        for (int ti = 0; ti < C::MT2; ++ti) {
+            uint32_t r[32];
+            tc::tmem_ld32(lane_base + 32 * ti, r);
+            tc::tmem_ld_wait();
+            if (!(look1 || look2)) continue;
+            const uint32_t bits = xin ? 0u : (ti == 0 ? mb.m[0] : ti == 1 ? mb.m[1] : mb.m[2]);
+            const int k2 = 16 * ti + (w.wt >> 3);
+#pragma unroll
+            for (int k1 = 0; k1 < 16; ++k1) {
+                if (!((bits >> k1) & 1u)) continue;
+                const float v1 = __uint_as_float(r[2 * k1]), v2 = __uint_as_float(r[2 * k1 + 1]);
+                if (!((look1 && v1 == M1) || (look2 && v2 == M2))) continue;
+                const int y = C::Pfa::map_coord(k1, k2);
+                const int Y = y + h < L ? y + h : y - h;
+                const int idx = Y * L + X;
+                if (look1 && v1 == M1) i1 = min(i1, idx);
+                if (look2 && v2 == M2) i2 = min(i2, idx);
+            }
+        }
+        if (i1 != 0x7fffffff) ka = argmax_key(M1, i1);
+        if (i2 != 0x7fffffff) kb = argmax_key(M2, i2);
     }
     const double d2a = warp_sum((double)s2a), d2b = warp_sum((double)s2b);
     ka = warp_max_u64(ka);
@@ -490,6 +531,7 @@ __global__ void __launch_bounds__(Tc2Cfg<kProducts>::kThreads, 1) k_corr_tc2(Tc2
     w.bar = bars + w.g;
     w.tmem = *tslot + (uint32_t)w.g * C::tmem_cols;
     w.ish = reinterpret_cast<int*>(sm + C::off_misc + 16) + 4 * w.g;
+    const Tc2Masks ymask = tc2_row_masks<C>(w.wt, a.yb0, a.yb1);
     const int total = (a.nu + a.lag) * 2 * C::T;
     if (w.wt == 0) {
         const int first = atomicAdd(a.next_item, 1);
@@ -524,7 +566,7 @@ __global__ void __launch_bounds__(Tc2Cfg<kProducts>::kThreads, 1) k_corr_tc2(Tc2
                 ok &= tc2_gemm<C, false, true>(w, sm, phase, a.error);
                 tc2_transition<C>(w);
                 ok &= tc2_gemm<C, true, true>(w, sm, phase, a.error);
-                tc2_col_out<C>(a, u, j - C::T, w);
+                tc2_col_out<C>(a, u, j - C::T, w, ymask);
                 __syncwarp();
                 if ((threadIdx.x & 31) == 0) {
                     int prev;
