@@ -71,7 +71,8 @@ struct Tc2Cfg {
     static constexpr int K2 = 32;               // stage 2: K = N = 2 x 16
     static constexpr int kWg = 5;               // pipelines per CTA
     static constexpr int kThreads = 128 * kWg;
-    static constexpr int kDone = 4 * T;         // warp completions per pass of a unit
+    static constexpr int kDone = T;             // tile completions per pass of a unit
+    static constexpr int kBatch = 4;            // items claimed (and published) together
     // stage-1 operand, row pass: K-major, 8-row groups 128 B apart, 8-element
     // K groups LBO1R apart (padded so that a warp's 4-byte stores of 32
     // consecutive columns hit distinct banks)
@@ -234,39 +235,61 @@ __device__ __forceinline__ void tc2_transition(const Tc2Wg& w) {
     }
 }
 
-// Row tile t of unit u: spectrum rows spectrum_row(8 t + v), product with the
-// pair spectrum, scaled, into A1 (row pass layout).
+// Per-thread constants of the row fill: column chunk i of warp w covers
+// columns c = 32 (w + 4 i) + lane (23 chunks per row, the last 16 wide); its
+// A1 offset (row group n1, K position (n2, re/im)) without the row v, and
+// whether the column exists.
+struct Tc2FillMap {
+    uint32_t off[6];
+    uint32_t valid;  // bit i
+};
 template <class C>
-__device__ __forceinline__ void tc2_row_fill(const Tc2Args& a, int u, int t, const Tc2Wg& w, float s) {
-    const int2 wp = __ldg(a.unit_wp + u);
-    const float2* Wr = a.W + (long long)wp.x * a.L2;
-    const float2* Pr = a.P + (long long)wp.y * a.L2;
-    const unsigned long long keep = l2_policy_evict_last();
-    const int warp = w.wt >> 5, lane = w.wt & 31;
-    // 32-column chunks: warp w takes chunks j = w, w + 4, ... (23 per row, the
-    // last 16 wide) of all 8 rows, so a lane's column, its prime-factor
-    // indices and its shared-memory offset serve 8 values, and the 16 loads
-    // of a chunk are in flight together
-    int srow[C::V];
+__device__ __forceinline__ Tc2FillMap tc2_fill_map(int wt) {
+    Tc2FillMap f;
+    f.valid = 0u;
+    const int warp = wt >> 5, lane = wt & 31;
 #pragma unroll
-    for (int v = 0; v < C::V; ++v) srow[v] = C::Pfa::spectrum_row(8 * t + v) * C::L;
-    for (int j = warp; j < 23; j += 4) {
-        const int c = 32 * j + lane;
-        if (c >= C::L) continue;
+    for (int i = 0; i < 6; ++i) {
+        const int c = 32 * (warp + 4 * i) + lane;
         const int n1 = c / C::N2, n2 = c - n1 * C::N2;
-        unsigned char* dst = w.a + (uint32_t)(n2 >> 2) * C::LBO1R + (uint32_t)n1 * 128 + (uint32_t)(n2 & 3) * 4;
-        float2 wv[C::V], pv[C::V];
+        f.off[i] = (uint32_t)(n2 >> 2) * C::LBO1R + (uint32_t)n1 * 128 + (uint32_t)(n2 & 3) * 4;
+        if (c < C::L) f.valid |= 1u << i;
+    }
+    return f;
+}
+
+// Row tile t of unit u: spectrum rows spectrum_row(8 t + v), product with the
+// pair spectrum, scaled, into A1 (row pass layout: row m = v + 8 n1 of the
+// operand is 8-row group n1, row v in it).  Row by row, the six column
+// chunks of a row are loaded together (one base pointer per row, the chunks
+// at fixed offsets) before any is used.
+template <class C>
+__device__ __forceinline__ void tc2_row_fill(const Tc2Args& a, int u, int t, const Tc2Wg& w, float s,
+                                             const Tc2FillMap& fm) {
+    const int2 wp = __ldg(a.unit_wp + u);
+    const int warp = w.wt >> 5, lane = w.wt & 31;
+    const float2* Wr = a.W + (long long)wp.x * a.L2 + 32 * warp + lane;
+    const float2* Pr = a.P + (long long)wp.y * a.L2 + 32 * warp + lane;
+    const unsigned long long keep = l2_policy_evict_last();
+#pragma unroll 1
+    for (int v = 0; v < C::V; ++v) {
+        const int row = C::Pfa::spectrum_row(8 * t + v) * C::L;
+        const float2* pw = Wr + row;
+        const float2* pp = Pr + row;
+        float2 wv[6], pv[6];
 #pragma unroll
-        for (int v = 0; v < C::V; ++v) {
-            wv[v] = ld_l2hint(Wr + srow[v] + c, keep);
-            pv[v] = __ldg(Pr + srow[v] + c);
-        }
+        for (int i = 0; i < 6; ++i)
+            if ((fm.valid >> i) & 1u) {
+                wv[i] = ld_l2hint(pw + 128 * i, keep);
+                pv[i] = __ldg(pp + 128 * i);
+            }
+        unsigned char* dst = w.a + (uint32_t)v * 16;
 #pragma unroll
-        for (int v = 0; v < C::V; ++v) {
-            const float2 x = cmulc(wv[v], pv[v]);
-            // row m = v + 8 n1 of the operand: 8-row group n1, row v in it
-            *reinterpret_cast<uint32_t*>(dst + (uint32_t)v * 16) = pack_half2(x.x * s, x.y * s);
-        }
+        for (int i = 0; i < 6; ++i)
+            if ((fm.valid >> i) & 1u) {
+                const float2 x = cmulc(wv[i], pv[i]);
+                *reinterpret_cast<uint32_t*>(dst + fm.off[i]) = pack_half2(x.x * s, x.y * s);
+            }
     }
     // K padding n2 = 45 .. 47 (K group 11, entries 1 .. 3): zero (their B rows are zero too)
     for (int i = w.wt; i < 128 * 3; i += 128) {
@@ -505,6 +528,25 @@ __device__ __forceinline__ void tc2_wait_for(const Tc2Args& a, int item) {
     }
 }
 
+// Count one finished tile (leader thread, after a __threadfence that orders
+// the pipeline's earlier stores and atomics before it); the last column tile
+// of a unit computes its scores.
+template <class C>
+__device__ __forceinline__ void tc2_publish(const Tc2Args& a, int item) {
+    const int s = item / (2 * C::T), j = item - s * (2 * C::T);
+    if (j < C::T) {
+        if (s < a.nu) atomicAdd(&a.done_rows[s], 1);
+        return;
+    }
+    const int u = s - a.lag;
+    if (u < 0 || u >= a.nu) return;
+    const int prev = atomicAdd(&a.done_cols[u], 1);
+    if (prev == C::kDone - 1) {
+        __threadfence();  // the other pipelines' accumulator atomics, published before their counts
+        tc2_finish_unit<C>(a, u);
+    }
+}
+
 template <int kProducts>
 __global__ void __launch_bounds__(Tc2Cfg<kProducts>::kThreads, 1) k_corr_tc2(Tc2Args a) {
     using C = Tc2Cfg<kProducts>;
@@ -532,32 +574,40 @@ __global__ void __launch_bounds__(Tc2Cfg<kProducts>::kThreads, 1) k_corr_tc2(Tc2
     w.tmem = *tslot + (uint32_t)w.g * C::tmem_cols;
     w.ish = reinterpret_cast<int*>(sm + C::off_misc + 16) + 4 * w.g;
     const Tc2Masks ymask = tc2_row_masks<C>(w.wt, a.yb0, a.yb1);
+    const Tc2FillMap fmap = tc2_fill_map<C>(w.wt);
     const int total = (a.nu + a.lag) * 2 * C::T;
+    // The pipeline leader claims batches of kBatch consecutive items (one
+    // atomic per batch), the pipeline processes them in order and the leader
+    // publishes the whole batch after its last item (one release for all of
+    // them, after the barrier that orders every warp's stores and
+    // accumulator atomics before it).  Deferring within a batch cannot
+    // deadlock: an item's dependency lies at least (lag - 1) x 2T items
+    // earlier, far more than a batch spans, so no item waits for another item
+    // of its own batch, and the earliest unpublished item's pipeline always
+    // gets through the rest of its batch.
+    int batch = 0, pre = 0;
     if (w.wt == 0) {
-        const int first = atomicAdd(a.next_item, 1);
-        if (first < total) tc2_wait_for<C>(a, first);
-        w.ish[0] = first;
+        batch = atomicAdd(a.next_item, C::kBatch);
+        if (batch < total) tc2_wait_for<C>(a, batch);
+        w.ish[0] = batch;
     }
     tc2_sync(w.g);
     uint32_t phase = 0;
     bool ok = true;
     int item = w.ish[0];
     for (int iter = 1; item < total; ++iter) {
-        int nxt = 0;
-        if (w.wt == 0) nxt = atomicAdd(a.next_item, 1);
+        const bool last_of_batch = (item - batch == C::kBatch - 1) || (item + 1 >= total);
+        if (w.wt == 0 && last_of_batch) pre = atomicAdd(a.next_item, C::kBatch);  // used after this item
         const int s = item / (2 * C::T), j = item - s * (2 * C::T);
         if (j < C::T) {
             if (s < a.nu) {
                 const int2 wp = __ldg(a.unit_wp + s);
                 const float sc = tc2_scale(__ldg(a.wmax + wp.x), __ldg(a.pmax + wp.y));
-                tc2_row_fill<C>(a, s, j, w, sc);
+                tc2_row_fill<C>(a, s, j, w, sc, fmap);
                 ok &= tc2_gemm<C, false, false>(w, sm, phase, a.error);
                 tc2_transition<C>(w);
                 ok &= tc2_gemm<C, true, false>(w, sm, phase, a.error);
                 tc2_row_out<C>(a, s, j, w);
-                __syncwarp();
-                if ((threadIdx.x & 31) == 0)
-                    asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(&a.done_rows[s]) : "memory");
             }
         } else {
             const int u = s - a.lag;
@@ -567,16 +617,19 @@ __global__ void __launch_bounds__(Tc2Cfg<kProducts>::kThreads, 1) k_corr_tc2(Tc2
                 tc2_transition<C>(w);
                 ok &= tc2_gemm<C, true, true>(w, sm, phase, a.error);
                 tc2_col_out<C>(a, u, j - C::T, w, ymask);
-                __syncwarp();
-                if ((threadIdx.x & 31) == 0) {
-                    int prev;
-                    asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;"
-                                 : "=r"(prev) : "l"(&a.done_cols[u]) : "memory");
-                    if (prev == C::kDone - 1) tc2_finish_unit<C>(a, u);
-                }
+            }
+        }
+        if (last_of_batch) {
+            // every warp's stores and atomics of the batch before the release
+            tc2_sync(w.g);
+            if (w.wt == 0) {
+                __threadfence();
+                for (int q = batch; q <= item; ++q) tc2_publish<C>(a, q);
+                batch = pre;
             }
         }
         if (w.wt == 0) {
+            const int nxt = last_of_batch ? batch : item + 1;
             if (nxt < total) tc2_wait_for<C>(a, nxt);
             w.ish[iter & 3] = nxt;
         }
