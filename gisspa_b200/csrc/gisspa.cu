@@ -1169,6 +1169,11 @@ static int corr_launch(gs_ctx* ctx, const float2* W, const float2* TS, int nu, c
     if (ctx->p.precision == GS_PREC_FP32) return launch_corr(ctx, l, t.tile, ca);
     if (ctx->p.precision == GS_PREC_TC_FULL || ctx->p.precision == GS_PREC_TC_FULL_1P) {
         if (l != 720) return set_err(ctx, GS_ERR_UNSUPPORTED, "the all-tensor-core path takes window 720 (got %d)", l);
+        // items are claimed and published in batches of 4: every dependency
+        // must lie more than a batch back (lag >= 1, slots >= lag + 2)
+        if (ca.lag < 1 || ca.S < ca.lag + 2)
+            return set_err(ctx, GS_ERR_UNSUPPORTED, "the all-tensor-core path needs lag >= 1 and slots >= lag + 2 "
+                           "(got lag %d, slots %d)", ca.lag, ca.S);
         Tc2Args a;
         a.W = ca.W; a.P = ca.P;
         a.R = P<__half2>(ctx->scratch);

@@ -585,18 +585,21 @@ __global__ void __launch_bounds__(Tc2Cfg<kProducts>::kThreads, 1) k_corr_tc2(Tc2
     // earlier, far more than a batch spans, so no item waits for another item
     // of its own batch, and the earliest unpublished item's pipeline always
     // gets through the rest of its batch.
-    int batch = 0, pre = 0;
+    // Claims start at 0 and advance by kBatch, so a batch starts at a
+    // multiple of kBatch: every thread tells the batch's last item from the
+    // item index alone (the extra barrier below must be taken by all).
+    int pre = 0;  // the leader's claim of the next batch
     if (w.wt == 0) {
-        batch = atomicAdd(a.next_item, C::kBatch);
-        if (batch < total) tc2_wait_for<C>(a, batch);
-        w.ish[0] = batch;
+        const int first = atomicAdd(a.next_item, C::kBatch);
+        if (first < total) tc2_wait_for<C>(a, first);
+        w.ish[0] = first;
     }
     tc2_sync(w.g);
     uint32_t phase = 0;
     bool ok = true;
     int item = w.ish[0];
     for (int iter = 1; item < total; ++iter) {
-        const bool last_of_batch = (item - batch == C::kBatch - 1) || (item + 1 >= total);
+        const bool last_of_batch = (item % C::kBatch == C::kBatch - 1) || (item + 1 >= total);
         if (w.wt == 0 && last_of_batch) pre = atomicAdd(a.next_item, C::kBatch);  // used after this item
         const int s = item / (2 * C::T), j = item - s * (2 * C::T);
         if (j < C::T) {
@@ -624,12 +627,11 @@ __global__ void __launch_bounds__(Tc2Cfg<kProducts>::kThreads, 1) k_corr_tc2(Tc2
             tc2_sync(w.g);
             if (w.wt == 0) {
                 __threadfence();
-                for (int q = batch; q <= item; ++q) tc2_publish<C>(a, q);
-                batch = pre;
+                for (int q = item - item % C::kBatch; q <= item; ++q) tc2_publish<C>(a, q);
             }
         }
         if (w.wt == 0) {
-            const int nxt = last_of_batch ? batch : item + 1;
+            const int nxt = last_of_batch ? pre : item + 1;
             if (nxt < total) tc2_wait_for<C>(a, nxt);
             w.ish[iter & 3] = nxt;
         }
