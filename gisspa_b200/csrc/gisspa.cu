@@ -79,6 +79,7 @@ struct gs_ctx {
     bool two_pass = false;
     int window_block = 4;
     int corr_slots = 16, corr_lag = 6;
+    bool corr_ring_set = false;        // slots / lag set through gs_set_option
     int corr_ctas = 0;                 // resident CTAs per SM of the persistent kernels (0 = as many as fit)
     int corr_tile = 16;                // vectors per tile of the FP32 persistent kernel (16 or 8)
     int corr_ctas_override = 0;        // value used by the launch in progress
@@ -89,6 +90,7 @@ struct gs_ctx {
     unsigned long long graph_kernel_launches = 0;
     DBuf unit_wp, dep_counters, pacc, flags;
     DBuf tc2_wmax, tc2_pmax;  // per window / per pair max |spectrum| (all-tensor-core path)
+    DBuf tc2_w16, tc2_p16;    // their FP16 copies, scaled by powers of two
     // off-grid refinement (refine.cuh): per-pick chunk buffers
     DBuf rf_pk, rf_acc, rf_B, rf_F1, rf_T, rf_TM, rf_F, rf_G, rf_TB, rf_mask;
     std::vector<cudaEvent_t> kev;  // pool of events for per-kernel timing
@@ -1179,6 +1181,8 @@ static int corr_launch(gs_ctx* ctx, const float2* W, const float2* TS, int nu, c
         a.R = P<__half2>(ctx->scratch);
         a.wmax = P<float>(ctx->tc2_wmax);
         a.pmax = P<float>(ctx->tc2_pmax);
+        a.W16 = P<__half2>(ctx->tc2_w16);
+        a.P16 = P<__half2>(ctx->tc2_p16);
         a.unit_wp = ca.unit_wp; a.done_rows = ca.done_rows; a.done_cols = ca.done_cols;
         a.acc = ca.acc; a.out = ca.out; a.next_item = ca.next_item; a.error = ca.error;
         a.nu = ca.nu; a.ntmpl = ca.ntmpl; a.S = ca.S; a.lag = ca.lag; a.L2 = ca.L2;
@@ -1294,6 +1298,13 @@ static int correlate_all(gs_ctx* ctx, float2* W, int NW, const std::vector<float
     FftPlan* plan = nullptr;
     TRY(get_plan(ctx, l, &plan));  // before any capture: plan creation copies synchronously
     CorrTuning tune{ctx->corr_slots, ctx->corr_lag, ctx->window_block, ctx->corr_ctas, ctx->corr_tile};
+    // the all-tensor-core kernel keeps about twice as many items in flight
+    // (five pipelines per SM, items claimed in pairs): its own defaults
+    // unless the caller set the ring explicitly
+    if (tc2 && !ctx->corr_ring_set) {
+        tune.slots = 24;
+        tune.lag = 12;
+    }
     // window spectra in PfaCols order for the duration of the correlation,
     // natural order again afterwards (on every return path)
     struct PfaWindows {
@@ -1319,9 +1330,12 @@ static int correlate_all(gs_ctx* ctx, float2* W, int NW, const std::vector<float
         // per-window max |W| for the FP16 scaling of each unit
         TRY(ensure(ctx, ctx->tc2_wmax, sizeof(float) * NW));
         TRY(ensure(ctx, ctx->tc2_pmax, sizeof(float) * Np));
+        TRY(ensure(ctx, ctx->tc2_w16, sizeof(__half2) * l2 * NW));
+        TRY(ensure(ctx, ctx->tc2_p16, sizeof(__half2) * l2 * Np));
         CK(cudaMemsetAsync(ctx->tc2_wmax.p, 0, sizeof(float) * NW, ctx->stream));
         k_max_abs<<<dim3(64, NW), 256, 0, ctx->stream>>>(W, l2, P<float>(ctx->tc2_wmax));
-        ++ctx->counters.kernel_launches;
+        k_to_half_scaled<<<dim3(64, NW), 256, 0, ctx->stream>>>(W, l2, P<float>(ctx->tc2_wmax), P<__half2>(ctx->tc2_w16));
+        ctx->counters.kernel_launches += 2;
         CKL();
     }
     if (persistent) {
@@ -1335,7 +1349,9 @@ static int correlate_all(gs_ctx* ctx, float2* W, int NW, const std::vector<float
             if (tc2) {
                 CK(cudaMemsetAsync(ctx->tc2_pmax.p, 0, sizeof(float) * Np, ctx->stream));
                 k_max_abs<<<dim3(64, Np), 256, 0, ctx->stream>>>(TS, l2, P<float>(ctx->tc2_pmax));
-                ++ctx->counters.kernel_launches;
+                k_to_half_scaled<<<dim3(64, Np), 256, 0, ctx->stream>>>(TS, l2, P<float>(ctx->tc2_pmax),
+                                                                       P<__half2>(ctx->tc2_p16));
+                ctx->counters.kernel_launches += 2;
                 CKL();
             }
             TRY(autotune(ctx, W, TS, NW, &tune));
@@ -1378,7 +1394,9 @@ static int correlate_all(gs_ctx* ctx, float2* W, int NW, const std::vector<float
         if (tc2) {
             CK(cudaMemsetAsync(ctx->tc2_pmax.p, 0, sizeof(float) * Np, ctx->stream));
             k_max_abs<<<dim3(64, Np), 256, 0, ctx->stream>>>(TS, l2, P<float>(ctx->tc2_pmax));
-            ++ctx->counters.kernel_launches;
+            k_to_half_scaled<<<dim3(64, Np), 256, 0, ctx->stream>>>(TS, l2, P<float>(ctx->tc2_pmax),
+                                                                   P<__half2>(ctx->tc2_p16));
+            ctx->counters.kernel_launches += 2;
             CKL();
         }
         if (rec) CK(cudaEventRecord(eb, ctx->stream));
@@ -1843,10 +1861,12 @@ int gs_set_option(gs_ctx* ctx, int option, int value) {
         case GS_OPT_CORR_SLOTS:
             if (value <= ctx->corr_lag) return set_err(ctx, GS_ERR_ARG, "slots must exceed the lag");
             ctx->corr_slots = value;
+            ctx->corr_ring_set = true;
             return GS_OK;
         case GS_OPT_CORR_LAG:
             if (value < 0 || value >= ctx->corr_slots) return set_err(ctx, GS_ERR_ARG, "lag must be in [0, slots)");
             ctx->corr_lag = value;
+            ctx->corr_ring_set = true;
             return GS_OK;
         case GS_OPT_WINDOW_BLOCK:
             if (value < 1) return set_err(ctx, GS_ERR_ARG, "window block must be >= 1");

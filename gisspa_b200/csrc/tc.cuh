@@ -114,6 +114,27 @@ __device__ __forceinline__ bool mbar_wait_suspend(uint64_t* bar, uint32_t parity
     }
 }
 
+// Waits until the barrier's phase with the given parity has completed,
+// polling with a short sleep in between (one thread, its warp issuing little
+// meanwhile); gives up after `limit_ns` of wall time (returns false).
+__device__ __forceinline__ bool mbar_wait_backoff(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
+    const uint32_t a = smem_u32(bar);
+    const uint64_t t0 = globaltimer_ns();
+    for (;;) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (globaltimer_ns() - t0 > limit_ns) return false;
+        __nanosleep(64);
+    }
+}
+
 // ---- fences ----
 // st.shared writes -> visible to the tensor core's (async proxy) reads
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }

@@ -42,6 +42,8 @@ namespace gs {
 struct Tc2Args {
     const float2* W;         // window spectra (PfaCols column order), Nw x L2
     const float2* P;         // template-pair spectra of this angle (PfaCols order), Np x L2
+    const __half2* W16;      // the same in FP16, each window scaled by its s_w (max |.| < 1)
+    const __half2* P16;      // the same in FP16, each pair scaled by its s_p
     __half2* R;              // scratch ring, S x L2 half2 (FP16 re, im in 8-column blocks)
     const float* wmax;       // per window max |W|
     const float* pmax;       // per pair max |P|
@@ -72,7 +74,7 @@ struct Tc2Cfg {
     static constexpr int kWg = 5;               // pipelines per CTA
     static constexpr int kThreads = 128 * kWg;
     static constexpr int kDone = T;             // tile completions per pass of a unit
-    static constexpr int kBatch = 4;            // items claimed (and published) together
+    static constexpr int kBatch = 2;            // items claimed (and published) together
     // stage-1 operand, row pass: K-major, 8-row groups 128 B apart, 8-element
     // K groups LBO1R apart (padded so that a warp's 4-byte stores of 32
     // consecutive columns hit distinct banks)
@@ -103,18 +105,37 @@ struct Tc2Cfg {
 struct Tc2Wg {
     int g, wt;            // pipeline, thread within it
     unsigned char* a;     // A1 / A2
+    uint32_t as;          // the same as a shared-window address
     uint64_t* bar;
     uint32_t tmem;
     int* ish;
 };
 
-// exact power-of-two scale s of a unit: max |W| max |P| s in (1/2, 1]
-__device__ __forceinline__ float tc2_scale(float wm, float pm) {
-    const float m = wm * pm;
+// Exact power-of-two scale of one spectrum from its max |.|: max |.| x s in
+// [1/2, 1) (1 for an all-zero or non-finite maximum).  A unit's map is
+// computed from the product of its window's and its pair's scaled spectra,
+// so its scale is s_w s_p and every intermediate stays below 45 x 720.
+__host__ __device__ __forceinline__ float tc2_scale1(float m) {
     if (!(m > 1e-30f) || !(m < 1e30f)) return 1.0f;
     int e;
-    frexpf(m, &e);          // m = f 2^e, f in [0.5, 1)
+    frexpf(m, &e);  // m = f 2^e, f in [0.5, 1)
     return ldexpf(1.0f, -e);
+}
+__device__ __forceinline__ float tc2_scale(float wm, float pm) { return tc2_scale1(wm) * tc2_scale1(pm); }
+
+// Stores to shared memory by 32-bit shared-window address.
+__device__ __forceinline__ void sts32(uint32_t addr, uint32_t v) {
+    asm volatile("st.shared.b32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+}
+// st.shared.b32 when `pred` is nonzero (predicated inside the instruction,
+// no branch around it).
+__device__ __forceinline__ void sts32_if(uint32_t addr, uint32_t v, uint32_t pred) {
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %2, 0;\n\t@p st.shared.b32 [%0], %1;\n\t}"
+                 ::"r"(addr), "r"(v), "r"(pred) : "memory");
+}
+__device__ __forceinline__ void sts128(uint32_t addr, uint4 v) {
+    asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w)
+                 : "memory");
 }
 
 __device__ __forceinline__ uint32_t pack_half2(float re, float im) {
@@ -156,17 +177,37 @@ __device__ void tc2_fill_dft(unsigned char* sm) {
     }
 }
 
-// Named barrier of one pipeline (ids 1 .. kWg; 0 is the CTA's).
-__device__ __forceinline__ void tc2_sync(int g) { asm volatile("bar.sync %0, 128;" ::"r"(g + 1) : "memory"); }
+// Named barrier of one pipeline (ids 1 .. kWg; 0 is the CTA's).  bar.sync is
+// the warp-aligned form: the warp is reconverged first (one lane may arrive
+// from a wait the others skipped).
+__device__ __forceinline__ void tc2_sync(int g) {
+    __syncwarp();
+    asm volatile("bar.sync %0, 128;" ::"r"(g + 1) : "memory");
+}
+
+// Bounded (about a second); gives up at once when another wait of the
+// launch has already given up (error flag set), so a failed launch ends soon.
+template <class C>
+__device__ __forceinline__ void tc2_wait_counter(const int* p, int target, int* error) {
+    if (ld_acquire_gpu(p) >= target) return;
+    for (int it = 0; it < (1 << 22); ++it) {
+        __nanosleep(256);
+        if (ld_acquire_gpu(p) >= target) return;
+        if ((it & 1023) == 1023 && *(volatile int*)error) return;
+    }
+    atomicExch(error, 1);
+}
 
 // Issue a GEMM stage (thread 0 of the pipeline), commit, wait for it (one
 // lane per warp polls the mbarrier).  Returns false when the bounded wait gave up.
 template <class C, bool kStage2, bool kColPass>
-__device__ __forceinline__ bool tc2_gemm(const Tc2Wg& w, unsigned char* sm, uint32_t& phase, const int* a_error) {
+__device__ __forceinline__ bool tc2_gemm(const Tc2Wg& w, unsigned char* sm, uint32_t& phase, int* a_error,
+                                         const int* dep = nullptr) {
     tc::fence_async_smem();
     tc::fence_before_sync();
     tc2_sync(w.g);
     tc::fence_after_sync();
+    int ok = 1;
     if (w.wt == 0) {
         const uint32_t a = tc::smem_u32(w.a);
         if (!kStage2) {
@@ -197,18 +238,23 @@ __device__ __forceinline__ bool tc2_gemm(const Tc2Wg& w, unsigned char* sm, uint
                                     (j | p) ? 1u : 0u);
         }
         tc::mma_commit(w.bar);
+        // a dependency to check after the MMAs: its acquire load is issued
+        // now, so that its round trip overlaps them
+        const int dv = dep ? ld_acquire_gpu(dep) : C::kDone;
+        // the issuing thread alone waits (sleeping between polls; bounded:
+        // 2 s, or 1 ms once any wait of the launch has given up); the other
+        // warps block on the barrier below and take no issue slots
+        const uint64_t limit = *(volatile const int*)a_error ? 1000000ull : 2000000000ull;
+        if (!tc::mbar_wait_backoff(w.bar, phase, limit)) {
+            ok = 0;
+            atomicExch(a_error, 1);
+        }
+        if (dv < C::kDone) tc2_wait_counter<C>(dep, C::kDone, a_error);
     }
-    __syncwarp();
-    int ok = 1;
-    // once any wait of the launch has given up, later waits end quickly
-    // lane 0 sleeps in try_wait until the MMAs complete (bounded: 2 s, or
-    // 1 ms once any wait of the launch has given up)
-    if ((threadIdx.x & 31) == 0)
-        ok = tc::mbar_wait_suspend(w.bar, phase, 100000u,
-                                   *(volatile int*)a_error ? 1000000ull : 2000000000ull) ? 1 : 0;
-    if (!ok && (threadIdx.x & 31) == 0) atomicExch(const_cast<int*>(a_error), 1);
-    ok = __shfl_sync(0xffffffffu, ok, 0);
     phase ^= 1u;
+    // the MMAs' completion, observed by the issuing thread, ordered before
+    // every thread's TMEM reads and operand rewrites
+    tc2_sync(w.g);
     tc::fence_after_sync();
     return ok != 0;
 }
@@ -220,7 +266,7 @@ __device__ __forceinline__ void tc2_transition(const Tc2Wg& w) {
     const int m = w.wt, v = m & 7, n1 = m >> 3;
     const uint32_t lane_base = w.tmem + ((uint32_t)(32 * (w.wt >> 5)) << 16);
     uint32_t r[32];
-    unsigned char* dst = w.a + (uint32_t)(n1 >> 2) * C::LBO2 + (uint32_t)v * 16 + (uint32_t)(n1 & 3) * 4;
+    const uint32_t dst = w.as + (uint32_t)(n1 >> 2) * C::LBO2 + (uint32_t)v * 16 + (uint32_t)(n1 & 3) * 4;
 #pragma unroll 1
     for (int q = 0; q < 3; ++q) {
         tc::tmem_ld32(lane_base + 32 * q, r);
@@ -229,19 +275,20 @@ __device__ __forceinline__ void tc2_transition(const Tc2Wg& w) {
         for (int i = 0; i < 16; ++i) {
             // A1 (aliased by A2) is no longer read: the stage-1 MMAs completed
             const int k2 = 16 * q + i;
-            *reinterpret_cast<uint32_t*>(dst + (uint32_t)k2 * 128) =
-                pack_half2(__uint_as_float(r[2 * i]), __uint_as_float(r[2 * i + 1]));
+            sts32(dst + (uint32_t)k2 * 128, pack_half2(__uint_as_float(r[2 * i]), __uint_as_float(r[2 * i + 1])));
         }
     }
 }
 
-// Per-thread constants of the row fill: column chunk i of warp w covers
-// columns c = 32 (w + 4 i) + lane (23 chunks per row, the last 16 wide); its
-// A1 offset (row group n1, K position (n2, re/im)) without the row v, and
-// whether the column exists.
+// Per-thread constants of the row fill: chunk i of warp w covers the column
+// pairs c = 64 (w + 4 i) + 2 lane, c + 1 (12 chunks of 64 columns per row,
+// the last 16 wide, so warp w takes chunks w, w + 4, w + 8); the A1 offsets
+// of both columns (row group n1, K position (n2, re/im)) without the row v,
+// and whether the pair exists.
 struct Tc2FillMap {
-    uint32_t off[6];
-    uint32_t valid;  // bit i
+    uint32_t off[6];  // [2 i + column of the pair]
+    uint32_t valid;   // bit i
+    int col[3];       // load offset of chunk i in column pairs (0 for a chunk past the row end)
 };
 template <class C>
 __device__ __forceinline__ Tc2FillMap tc2_fill_map(int wt) {
@@ -249,53 +296,64 @@ __device__ __forceinline__ Tc2FillMap tc2_fill_map(int wt) {
     f.valid = 0u;
     const int warp = wt >> 5, lane = wt & 31;
 #pragma unroll
-    for (int i = 0; i < 6; ++i) {
-        const int c = 32 * (warp + 4 * i) + lane;
-        const int n1 = c / C::N2, n2 = c - n1 * C::N2;
-        f.off[i] = (uint32_t)(n2 >> 2) * C::LBO1R + (uint32_t)n1 * 128 + (uint32_t)(n2 & 3) * 4;
-        if (c < C::L) f.valid |= 1u << i;
-    }
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int c = 64 * (warp + 4 * i) + 2 * lane + q;
+            const int n1 = c / C::N2, n2 = c - n1 * C::N2;
+            f.off[2 * i + q] = (uint32_t)(n2 >> 2) * C::LBO1R + (uint32_t)n1 * 128 + (uint32_t)(n2 & 3) * 4;
+            if (q == 0 && c < C::L) f.valid |= 1u << i;  // L is even: c < L implies c + 1 < L
+        }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) f.col[i] = ((f.valid >> i) & 1u) ? 32 * (warp + 4 * i) + lane : 0;
     return f;
 }
 
-// Row tile t of unit u: spectrum rows spectrum_row(8 t + v), product with the
-// pair spectrum, scaled, into A1 (row pass layout: row m = v + 8 n1 of the
-// operand is 8-row group n1, row v in it).  Row by row, the six column
-// chunks of a row are loaded together (one base pointer per row, the chunks
-// at fixed offsets) before any is used.
+// Row tile t of unit u: spectrum rows spectrum_row(8 t + v) of the FP16
+// window and pair spectra (each already scaled to max |.| < 1), their
+// product into A1 (row pass layout: row m = v + 8 n1 of the operand is
+// 8-row group n1, row v in it).  Four rounds of two rows, every load of a
+// round in flight together (8-byte loads of two columns).
 template <class C>
-__device__ __forceinline__ void tc2_row_fill(const Tc2Args& a, int u, int t, const Tc2Wg& w, float s,
-                                             const Tc2FillMap& fm) {
+__device__ __forceinline__ void tc2_row_fill(const Tc2Args& a, int u, int t, const Tc2Wg& w, const Tc2FillMap& fm) {
     const int2 wp = __ldg(a.unit_wp + u);
     const int warp = w.wt >> 5, lane = w.wt & 31;
-    const float2* Wr = a.W + (long long)wp.x * a.L2 + 32 * warp + lane;
-    const float2* Pr = a.P + (long long)wp.y * a.L2 + 32 * warp + lane;
+    const uint2* Wr = reinterpret_cast<const uint2*>(a.W16 + (long long)wp.x * a.L2);
+    const uint2* Pr = reinterpret_cast<const uint2*>(a.P16 + (long long)wp.y * a.L2);
     const unsigned long long keep = l2_policy_evict_last();
 #pragma unroll 1
-    for (int v = 0; v < C::V; ++v) {
-        const int row = C::Pfa::spectrum_row(8 * t + v) * C::L;
-        const float2* pw = Wr + row;
-        const float2* pp = Pr + row;
-        float2 wv[6], pv[6];
+    for (int v0 = 0; v0 < C::V; v0 += 2) {
+        uint2 wv[2][3], pv[2][3];
 #pragma unroll
-        for (int i = 0; i < 6; ++i)
-            if ((fm.valid >> i) & 1u) {
-                wv[i] = ld_l2hint(pw + 128 * i, keep);
-                pv[i] = __ldg(pp + 128 * i);
-            }
-        unsigned char* dst = w.a + (uint32_t)v * 16;
+        for (int r = 0; r < 2; ++r) {
+            const int row = C::Pfa::spectrum_row(8 * t + v0 + r) * (C::L / 2);  // in uint2 (column pairs)
+            // every lane loads (a chunk past the row end re-reads column 0)
 #pragma unroll
-        for (int i = 0; i < 6; ++i)
-            if ((fm.valid >> i) & 1u) {
-                const float2 x = cmulc(wv[i], pv[i]);
-                *reinterpret_cast<uint32_t*>(dst + fm.off[i]) = pack_half2(x.x * s, x.y * s);
+            for (int i = 0; i < 3; ++i) {
+                asm volatile("ld.global.L1::no_allocate.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;"
+                             : "=r"(wv[r][i].x), "=r"(wv[r][i].y) : "l"(Wr + row + fm.col[i]), "l"(keep));
+                pv[r][i] = __ldg(Pr + row + fm.col[i]);
             }
+        }
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const uint32_t dst = w.as + (uint32_t)(v0 + r) * 16;
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const uint32_t wq = q ? wv[r][i].y : wv[r][i].x, pq = q ? pv[r][i].y : pv[r][i].x;
+                    const float2 wf = __half22float2(*reinterpret_cast<const __half2*>(&wq));
+                    const float2 pf = __half22float2(*reinterpret_cast<const __half2*>(&pq));
+                    const float2 x = cmulc(wf, pf);
+                    sts32_if(dst + fm.off[2 * i + q], pack_half2(x.x, x.y), (fm.valid >> i) & 1u);
+                }
+        }
     }
     // K padding n2 = 45 .. 47 (K group 11, entries 1 .. 3): zero (their B rows are zero too)
     for (int i = w.wt; i < 128 * 3; i += 128) {
         const int m = i / 3, n2 = 45 + (i - (i / 3) * 3);
-        *reinterpret_cast<uint32_t*>(w.a + 11u * C::LBO1R + (uint32_t)(m >> 3) * 128 + (uint32_t)(m & 7) * 16 +
-                                     (uint32_t)(n2 & 3) * 4) = 0u;
+        sts32(w.as + 11u * C::LBO1R + (uint32_t)(m >> 3) * 128 + (uint32_t)(m & 7) * 16 + (uint32_t)(n2 & 3) * 4, 0u);
     }
 }
 
@@ -313,30 +371,25 @@ __device__ __forceinline__ void tc2_col_fill(const Tc2Args& a, int u, int t, con
     uint4 vals[kPer];
 #pragma unroll
     for (int i = 0; i < kPer; ++i) {
-        const int q = base + w.wt + 128 * i;
-        if (q < kChunks) {
-            const int r = q >> 1, h = q & 1;
-            const uint4* src = reinterpret_cast<const uint4*>(Rs + (long long)r * C::L + 8 * t) + h;
-            asm volatile("ld.global.L1::no_allocate.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
-                         : "=r"(vals[i].x), "=r"(vals[i].y), "=r"(vals[i].z), "=r"(vals[i].w)
-                         : "l"(src), "l"(drop));
-        }
+        const int q = min(base + w.wt + 128 * i, kChunks - 1);  // past the end: re-read the last chunk
+        const int r = q >> 1, h = q & 1;
+        const uint4* src = reinterpret_cast<const uint4*>(Rs + (long long)r * C::L + 8 * t) + h;
+        asm volatile("ld.global.L1::no_allocate.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+                     : "=r"(vals[i].x), "=r"(vals[i].y), "=r"(vals[i].z), "=r"(vals[i].w)
+                     : "l"(src), "l"(drop));
     }
 #pragma unroll
     for (int i = 0; i < kPer; ++i) {
-        const int q = base + w.wt + 128 * i;
-        if (q < kChunks) {
-            const int r = q >> 1, h = q & 1;
-            const int n1 = r / C::N2, n2 = r - n1 * C::N2;
-            *reinterpret_cast<uint4*>(w.a + (uint32_t)n1 * C::SBO1C + (uint32_t)n2 * 32 + (uint32_t)h * 16) = vals[i];
-        }
+        const int q = min(base + w.wt + 128 * i, kChunks - 1);  // a repeated chunk stores the same bytes again
+        const int r = q >> 1, h = q & 1;
+        const int n1 = r / C::N2, n2 = r - n1 * C::N2;
+        sts128(w.as + (uint32_t)n1 * C::SBO1C + (uint32_t)n2 * 32 + (uint32_t)h * 16, vals[i]);
     }
     }
     // K padding rows n2 = 45 .. 47 of every n1 group: zero
     for (int i = w.wt; i < 16 * 3 * 2; i += 128) {
         const int n1 = i / 6, rest = i - n1 * 6, n2 = 45 + (rest >> 1), h = rest & 1;
-        *reinterpret_cast<uint4*>(w.a + (uint32_t)n1 * C::SBO1C + (uint32_t)n2 * 32 + (uint32_t)h * 16) =
-            make_uint4(0u, 0u, 0u, 0u);
+        sts128(w.as + (uint32_t)n1 * C::SBO1C + (uint32_t)n2 * 32 + (uint32_t)h * 16, make_uint4(0u, 0u, 0u, 0u));
     }
 }
 
@@ -400,10 +453,10 @@ __device__ __forceinline__ Tc2Masks tc2_row_masks(int wt, int yb0, int yb1) {
 
 // Column-pass epilogue: values of map column x (physical column 8 t + v),
 // rows map_coord(k1, k2), both templates of the pair: the sum of squares and
-// the border-masked maximum (starting at 0, as the reference's peak) per
-// thread, the maximum reduced over the warp, and only the lanes holding the
-// warp's maximum look for its position (re-reading their TMEM lanes); the
-// warp then adds its share to the unit's accumulators.
+// the border-masked maximum (starting at 0, as the reference's peak) with its
+// position, per thread (the position as (tile, k1), k1 a compile-time
+// constant; among equal values the first in (tile, k1) order), then per warp
+// (smallest map index among equal values), added to the unit's accumulators.
 template <class C>
 __device__ __forceinline__ void tc2_col_out(const Tc2Args& a, int u, int t, const Tc2Wg& w, const Tc2Masks mb) {
     constexpr int L = C::L, h = L / 2;
@@ -412,8 +465,9 @@ __device__ __forceinline__ void tc2_col_out(const Tc2Args& a, int u, int t, cons
     const int pc = 8 * t + (w.wt & 7);                           // physical column
     const int x = C::Pfa::map_coord(pc & 15, pc >> 4);           // map column
     const bool xin = (unsigned)(x - a.yb0) <= (unsigned)(a.yb1 - a.yb0);  // column in the border
-    float m1 = 0.0f, m2 = 0.0f, s2a = 0.0f, s2b = 0.0f;
-    // the tile loops stay rolled: one 32-register array is live at a time
+    float b1 = 0.0f, b2 = 0.0f, s2a = 0.0f, s2b = 0.0f;
+    int k1a = -1, k1b = -1, tia = 0, tib = 0;
+    // the tile loop stays rolled: one 32-register array is live at a time
 #pragma unroll 1
     for (int ti = 0; ti < C::MT2; ++ti) {
         uint32_t r[32];
@@ -421,59 +475,48 @@ __device__ __forceinline__ void tc2_col_out(const Tc2Args& a, int u, int t, cons
         tc::tmem_ld_wait();
         // rows k2 >= 45 hold zeros and no bits
         const uint32_t bits = xin ? 0u : (ti == 0 ? mb.m[0] : ti == 1 ? mb.m[1] : mb.m[2]);
+        const float b1_0 = b1, b2_0 = b2;
 #pragma unroll
         for (int k1 = 0; k1 < 16; ++k1) {
             const float v1 = __uint_as_float(r[2 * k1]), v2 = __uint_as_float(r[2 * k1 + 1]);
             const bool in = (bits >> k1) & 1u;
-            m1 = fmaxf(m1, in ? v1 : 0.0f);
-            m2 = fmaxf(m2, in ? v2 : 0.0f);
+            const bool g1 = in && v1 > b1, g2 = in && v2 > b2;
+            b1 = g1 ? v1 : b1;
+            k1a = g1 ? k1 : k1a;
+            b2 = g2 ? v2 : b2;
+            k1b = g2 ? k1 : k1b;
             s2a = fmaf(v1, v1, s2a);
             s2b = fmaf(v2, v2, s2b);
         }
+        // the maximum only grows strictly: it changed iff it now lies in this tile
+        tia = b1 != b1_0 ? ti : tia;
+        tib = b2 != b2_0 ? ti : tib;
     }
-    float M1 = m1, M2 = m2;
+    const int X = x + h < L ? x + h : x - h;
+    auto key_of = [&](float b, int k1, int ti) -> unsigned long long {
+        if (k1 < 0) return 0ull;
+        const int k2 = 16 * ti + (w.wt >> 3);
+        const int y = C::Pfa::map_coord(k1, k2);
+        const int Y = y + h < L ? y + h : y - h;
+        return argmax_key(b, Y * L + X);
+    };
+    unsigned long long ka = key_of(b1, k1a, tia), kb = key_of(b2, k1b, tib);
+    float fa = s2a, fb = s2b;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        M1 = fmaxf(M1, __shfl_xor_sync(0xffffffffu, M1, o));
-        M2 = fmaxf(M2, __shfl_xor_sync(0xffffffffu, M2, o));
+        fa += __shfl_xor_sync(0xffffffffu, fa, o);
+        fb += __shfl_xor_sync(0xffffffffu, fb, o);
+        const unsigned long long oa = __shfl_xor_sync(0xffffffffu, ka, o);
+        const unsigned long long ob = __shfl_xor_sync(0xffffffffu, kb, o);
+        ka = oa > ka ? oa : ka;
+        kb = ob > kb ? ob : kb;
     }
-    unsigned long long ka = 0ull, kb = 0ull;
-    if (M1 > 0.0f || M2 > 0.0f) {   // warp-uniform: every lane re-reads its TMEM lanes
-        const bool look1 = M1 > 0.0f && m1 == M1, look2 = M2 > 0.0f && m2 == M2;
-        const int X = x + h < L ? x + h : x - h;
-        int i1 = 0x7fffffff, i2 = 0x7fffffff;
-#pragma unroll 1
-        for (int ti = 0; ti < C::MT2; ++ti) {
-            uint32_t r[32];
-            tc::tmem_ld32(lane_base + 32 * ti, r);
-            tc::tmem_ld_wait();
-            if (!(look1 || look2)) continue;
-            const uint32_t bits = xin ? 0u : (ti == 0 ? mb.m[0] : ti == 1 ? mb.m[1] : mb.m[2]);
-            const int k2 = 16 * ti + (w.wt >> 3);
-#pragma unroll
-            for (int k1 = 0; k1 < 16; ++k1) {
-                if (!((bits >> k1) & 1u)) continue;
-                const float v1 = __uint_as_float(r[2 * k1]), v2 = __uint_as_float(r[2 * k1 + 1]);
-                if (!((look1 && v1 == M1) || (look2 && v2 == M2))) continue;
-                const int y = C::Pfa::map_coord(k1, k2);
-                const int Y = y + h < L ? y + h : y - h;
-                const int idx = Y * L + X;
-                if (look1 && v1 == M1) i1 = min(i1, idx);
-                if (look2 && v2 == M2) i2 = min(i2, idx);
-            }
-        }
-        if (i1 != 0x7fffffff) ka = argmax_key(M1, i1);
-        if (i2 != 0x7fffffff) kb = argmax_key(M2, i2);
-    }
-    const double d2a = warp_sum((double)s2a), d2b = warp_sum((double)s2b);
-    ka = warp_max_u64(ka);
-    kb = warp_max_u64(kb);
     if ((threadIdx.x & 31) == 0) {
         UnitAcc* ac = a.acc + 2 * (long long)u;
         if (ka) atomicMax(&ac[0].key, ka);
-        atomicAdd(&ac[0].s2, d2a);
+        atomicAdd(&ac[0].s2, (double)fa);
         if (kb) atomicMax(&ac[1].key, kb);
-        atomicAdd(&ac[1].s2, d2b);
+        atomicAdd(&ac[1].s2, (double)fb);
     }
 }
 
@@ -503,29 +546,23 @@ __device__ __forceinline__ void tc2_finish_unit(const Tc2Args& a, int u) {
     }
 }
 
-// Bounded (about a second); gives up at once when another wait of the
-// launch has already given up (error flag set), so a failed launch ends soon.
-template <class C>
-__device__ __forceinline__ void tc2_wait_counter(const int* p, int target, int* error) {
-    if (ld_acquire_gpu(p) >= target) return;
-    for (int it = 0; it < (1 << 22); ++it) {
-        __nanosleep(256);
-        if (ld_acquire_gpu(p) >= target) return;
-        if ((it & 1023) == 1023 && *(volatile int*)error) return;
-    }
-    atomicExch(error, 1);
-}
-
-// Called by a pipeline's leader thread only; a pipeline barrier follows.
+// Called by a pipeline's leader thread only; a pipeline barrier follows.  A
+// column tile reads its unit's row maps, so it waits before the item; a row
+// tile needs its scratch slot only for its output, and checks that inside
+// its stage-2 GEMM (tc2_row_dep).
 template <class C>
 __device__ __forceinline__ void tc2_wait_for(const Tc2Args& a, int item) {
     const int s = item / (2 * C::T), j = item - s * (2 * C::T);
-    if (j < C::T) {
-        if (s < a.nu && s >= a.S) tc2_wait_counter<C>(a.done_cols + (s - a.S), C::kDone, a.error);
-    } else {
+    if (j >= C::T) {
         const int u = s - a.lag;
         if (u >= 0 && u < a.nu) tc2_wait_counter<C>(a.done_rows + u, C::kDone, a.error);
     }
+}
+// The counter a row tile of unit s waits for before writing slot s % S (the
+// column tiles of unit s - S), or nullptr.
+template <class C>
+__device__ __forceinline__ const int* tc2_row_dep(const Tc2Args& a, int s) {
+    return s >= a.S ? a.done_cols + (s - a.S) : nullptr;
 }
 
 // Count one finished tile (leader thread, after a __threadfence that orders
@@ -570,6 +607,7 @@ __global__ void __launch_bounds__(Tc2Cfg<kProducts>::kThreads, 1) k_corr_tc2(Tc2
     w.g = threadIdx.x >> 7;
     w.wt = threadIdx.x & 127;
     w.a = sm + C::off_a + (size_t)w.g * C::a_bytes;
+    w.as = tc::smem_u32(w.a);
     w.bar = bars + w.g;
     w.tmem = *tslot + (uint32_t)w.g * C::tmem_cols;
     w.ish = reinterpret_cast<int*>(sm + C::off_misc + 16) + 4 * w.g;
@@ -600,16 +638,15 @@ __global__ void __launch_bounds__(Tc2Cfg<kProducts>::kThreads, 1) k_corr_tc2(Tc2
     int item = w.ish[0];
     for (int iter = 1; item < total; ++iter) {
         const bool last_of_batch = (item % C::kBatch == C::kBatch - 1) || (item + 1 >= total);
-        if (w.wt == 0 && last_of_batch) pre = atomicAdd(a.next_item, C::kBatch);  // used after this item
+        // the next batch is claimed at this batch's first item, well before it is needed
+        if (w.wt == 0 && item % C::kBatch == 0) pre = atomicAdd(a.next_item, C::kBatch);
         const int s = item / (2 * C::T), j = item - s * (2 * C::T);
         if (j < C::T) {
             if (s < a.nu) {
-                const int2 wp = __ldg(a.unit_wp + s);
-                const float sc = tc2_scale(__ldg(a.wmax + wp.x), __ldg(a.pmax + wp.y));
-                tc2_row_fill<C>(a, s, j, w, sc, fmap);
+                tc2_row_fill<C>(a, s, j, w, fmap);
                 ok &= tc2_gemm<C, false, false>(w, sm, phase, a.error);
                 tc2_transition<C>(w);
-                ok &= tc2_gemm<C, true, false>(w, sm, phase, a.error);
+                ok &= tc2_gemm<C, true, false>(w, sm, phase, a.error, tc2_row_dep<C>(a, s));
                 tc2_row_out<C>(a, s, j, w);
             }
         } else {
@@ -647,6 +684,19 @@ __global__ void __launch_bounds__(Tc2Cfg<kProducts>::kThreads, 1) k_corr_tc2(Tc2
     __syncthreads();
     tc::fence_after_sync();
     if ((threadIdx.x >> 5) == 0) tc::tmem_dealloc(*tslot, 512);
+}
+
+// FP16 copy of `count` images of l2 complex values, image i scaled by the
+// exact power of two tc2_scale1(maxabs[i]).
+__global__ void k_to_half_scaled(const float2* __restrict__ z, long long l2, const float* __restrict__ maxabs,
+                                 __half2* __restrict__ out) {
+    const float s = tc2_scale1(__ldg(maxabs + blockIdx.y));
+    const float2* img = z + (long long)blockIdx.y * l2;
+    __half2* o = out + (long long)blockIdx.y * l2;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < l2; i += (long long)gridDim.x * blockDim.x) {
+        const float2 v = img[i];
+        o[i] = __floats2half2_rn(v.x * s, v.y * s);
+    }
 }
 
 // Per-row-block maximum of |z| of `count` images of l2 complex values each,
