@@ -565,7 +565,7 @@ __device__ __forceinline__ const int* tc2_row_dep(const Tc2Args& a, int s) {
     return s >= a.S ? a.done_cols + (s - a.S) : nullptr;
 }
 
-// Count one finished tile (leader thread, after a __threadfence that orders
+// Count one finished tile (leader thread, after a release fence that orders
 // the pipeline's earlier stores and atomics before it); the last column tile
 // of a unit computes its scores.
 template <class C>
@@ -579,7 +579,8 @@ __device__ __forceinline__ void tc2_publish(const Tc2Args& a, int item) {
     if (u < 0 || u >= a.nu) return;
     const int prev = atomicAdd(&a.done_cols[u], 1);
     if (prev == C::kDone - 1) {
-        __threadfence();  // the other pipelines' accumulator atomics, published before their counts
+        // acquire: the other pipelines' accumulator atomics, published before their counts
+        asm volatile("fence.acq_rel.gpu;" ::: "memory");
         tc2_finish_unit<C>(a, u);
     }
 }
@@ -663,7 +664,9 @@ __global__ void __launch_bounds__(Tc2Cfg<kProducts>::kThreads, 1) k_corr_tc2(Tc2
             // every warp's stores and atomics of the batch before the release
             tc2_sync(w.g);
             if (w.wt == 0) {
-                __threadfence();
+                // release: the batch's stores and atomics (ordered before by
+                // the barrier) before its counts
+                asm volatile("fence.acq_rel.gpu;" ::: "memory");
                 for (int q = item - item % C::kBatch; q <= item; ++q) tc2_publish<C>(a, q);
             }
         }

@@ -2,8 +2,9 @@
 200^2, 72 angles, window 720, overlap 200: 12.67 M units) on a subset of
 units, against the FP64 oracle: every unit of a few seeded (template, angle)
 pairs in all 88 windows, plus seeded units among those whose score reaches the
-pick threshold.  Run for the FP32 path (scores within SCORE_RTOL) and for both
-tensor-core precisions (split BF16 and split FP16 DFT stage, scores within
+pick threshold.  Run for the FP32 path (scores within SCORE_RTOL) and for the
+tensor-core precisions (split BF16 and split FP16 45-point stage; every DFT
+stage in FP16 with the DFT matrix split or rounded once; scores within
 TC_SCORE_RTOL, the bound stated for that path).  Positions equal unless the
 oracle's own map holds a value within 1e-5 of its peak at the GPU's position
 (a tie at FP32 resolution).  The oracle side is computed once and shared by
@@ -116,8 +117,10 @@ def _oracle_units():
 
 @pytest.mark.parametrize("precision,rtol", [(G.GS_PREC_FP32, H.SCORE_RTOL),
                                             (G.GS_PREC_TC_BF16, TC_SCORE_RTOL),
-                                            (G.GS_PREC_TC_FP16, TC_SCORE_RTOL)],
-                         ids=["fp32", "tc_bf16", "tc_fp16"])
+                                            (G.GS_PREC_TC_FP16, TC_SCORE_RTOL),
+                                            (G.GS_PREC_TC_FULL, TC_SCORE_RTOL),
+                                            (G.GS_PREC_TC_FULL_1P, TC_SCORE_RTOL)],
+                         ids=["fp32", "tc_bf16", "tc_fp16", "tc_full", "tc_full_1p"])
 def test_full_size_units_match_oracle(precision, rtol):
     ref = _oracle_units()
     u = _search_units(precision)
