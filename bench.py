@@ -325,15 +325,18 @@ def tensor_core_comparison(ds, kw, local_rank, base_precision: str):
         r["micrographs_per_s_at_72_angles"] = 1000.0 / (r["micrograph_prep_plus_spectra_per_angle_ms"]
                                                         + 72 * r["per_angle_correlation_ms"])
         res[name] = r
-    key = lambda p: (int(p["angle_index"]), int(p["window_x"]), int(p["window_y"]),
-                     int(p["template_index"]), float(p["center_x"]), float(p["center_y"]))
+    # a pick is a (angle, window, template) unit at or above the threshold; its
+    # peak may move between near-equal pixels (counted separately)
+    key = lambda p: (int(p["angle_index"]), int(p["window_x"]), int(p["window_y"]), int(p["template_index"]))
     out = {"angles_timed": 3, "note": "same micrograph and templates as the headline; per-angle times "
            "extrapolated to 72 angles for the micrographs/s of each path", "threshold": thres}
     base = {key(p): float(p["score"]) for p in picks.get("fp32", [])}
+    base_c = {key(p): (float(p["center_x"]), float(p["center_y"])) for p in picks.get("fp32", [])}
     for name in names:
         r = dict(res[name])
         if name != "fp32" and "error" not in r and "fp32" in picks:
             other = {key(p): float(p["score"]) for p in picks[name]}
+            other_c = {key(p): (float(p["center_x"]), float(p["center_y"])) for p in picks[name]}
             common = set(base) & set(other)
             only = set(base) ^ set(other)
             sc = [base.get(k, other.get(k)) for k in only]
@@ -343,6 +346,7 @@ def tensor_core_comparison(ds, kw, local_rank, base_precision: str):
             r["picks_differing"] = len(only)
             r["differing_picks_within_1e-3_of_threshold"] = all(abs(x - thres) <= 1e-3 * abs(thres) for x in sc)
             r["max_rel_score_diff"] = max([abs(base[k] - other[k]) / abs(base[k]) for k in common], default=0.0)
+            r["peaks_moved"] = sum(base_c[k] != other_c[k] for k in common)
         out[name.replace("-", "_")] = r
     done = [n for n in names[1:] if "speed_over_fp32" in out[n.replace("-", "_")]]
     if done:

@@ -7,7 +7,7 @@ tensor-core precisions (split BF16 and split FP16 45-point stage; every DFT
 stage in FP16 with the DFT matrix split or rounded once; scores within
 TC_SCORE_RTOL, the bound stated for that path).  Positions equal unless the
 oracle's own map holds a value within 1e-5 of its peak at the GPU's position
-(a tie at FP32 resolution).  The oracle side is computed once and shared by
+(a tie at FP32 resolution; within TC_SCORE_RTOL for the tensor-core paths).  The oracle side is computed once and shared by
 the three precisions.  GISSPA_SLOW=1 widens the subset about four-fold."""
 import os
 
@@ -134,8 +134,11 @@ def test_full_size_units_match_oracle(precision, rtol):
         n += 1
         worst = max(worst, abs(got_s - ref_s) / abs(ref_s))
         if got_p != ref_p:
+            # a tie at the path's resolution: the oracle's own map holds a
+            # value within the path's tolerance of its peak at the GPU's position
             peak = masked[ref_p]
-            assert masked[got_p] >= peak - 1e-5 * abs(peak), (ai, w, J, got_p, ref_p)
+            tie = 1e-5 if precision == G.GS_PREC_FP32 else rtol
+            assert masked[got_p] >= peak - tie * abs(peak), (ai, w, J, got_p, ref_p)
             ties += 1
     print("full-size subset, precision %d: %d units (%d pairs x 88 windows + threshold units), "
           "worst score error %.2e, %d near-tie positions" % (precision, n, N_PAIRS, worst, ties))
