@@ -1330,11 +1330,12 @@ static int correlate_all(gs_ctx* ctx, float2* W, int NW, const std::vector<float
         // per-window max |W| for the FP16 scaling of each unit
         TRY(ensure(ctx, ctx->tc2_wmax, sizeof(float) * NW));
         TRY(ensure(ctx, ctx->tc2_pmax, sizeof(float) * Np));
-        TRY(ensure(ctx, ctx->tc2_w16, sizeof(__half2) * l2 * NW));
-        TRY(ensure(ctx, ctx->tc2_p16, sizeof(__half2) * l2 * Np));
+        // FP16 copies in the row tiles' order: l rows of 16 x 48 values
+        TRY(ensure(ctx, ctx->tc2_w16, sizeof(__half2) * (size_t)l * 768 * NW));
+        TRY(ensure(ctx, ctx->tc2_p16, sizeof(__half2) * (size_t)l * 768 * Np));
         CK(cudaMemsetAsync(ctx->tc2_wmax.p, 0, sizeof(float) * NW, ctx->stream));
         k_max_abs<<<dim3(64, NW), 256, 0, ctx->stream>>>(W, l2, P<float>(ctx->tc2_wmax));
-        k_to_half_scaled<<<dim3(64, NW), 256, 0, ctx->stream>>>(W, l2, P<float>(ctx->tc2_wmax), P<__half2>(ctx->tc2_w16));
+        k_to_half_tiles<<<dim3(64, NW), 256, 0, ctx->stream>>>(W, P<float>(ctx->tc2_wmax), P<__half2>(ctx->tc2_w16));
         ctx->counters.kernel_launches += 2;
         CKL();
     }
@@ -1349,8 +1350,8 @@ static int correlate_all(gs_ctx* ctx, float2* W, int NW, const std::vector<float
             if (tc2) {
                 CK(cudaMemsetAsync(ctx->tc2_pmax.p, 0, sizeof(float) * Np, ctx->stream));
                 k_max_abs<<<dim3(64, Np), 256, 0, ctx->stream>>>(TS, l2, P<float>(ctx->tc2_pmax));
-                k_to_half_scaled<<<dim3(64, Np), 256, 0, ctx->stream>>>(TS, l2, P<float>(ctx->tc2_pmax),
-                                                                       P<__half2>(ctx->tc2_p16));
+                k_to_half_tiles<<<dim3(64, Np), 256, 0, ctx->stream>>>(TS, P<float>(ctx->tc2_pmax),
+                                                                      P<__half2>(ctx->tc2_p16));
                 ctx->counters.kernel_launches += 2;
                 CKL();
             }
@@ -1394,8 +1395,8 @@ static int correlate_all(gs_ctx* ctx, float2* W, int NW, const std::vector<float
         if (tc2) {
             CK(cudaMemsetAsync(ctx->tc2_pmax.p, 0, sizeof(float) * Np, ctx->stream));
             k_max_abs<<<dim3(64, Np), 256, 0, ctx->stream>>>(TS, l2, P<float>(ctx->tc2_pmax));
-            k_to_half_scaled<<<dim3(64, Np), 256, 0, ctx->stream>>>(TS, l2, P<float>(ctx->tc2_pmax),
-                                                                   P<__half2>(ctx->tc2_p16));
+            k_to_half_tiles<<<dim3(64, Np), 256, 0, ctx->stream>>>(TS, P<float>(ctx->tc2_pmax),
+                                                                  P<__half2>(ctx->tc2_p16));
             ctx->counters.kernel_launches += 2;
             CKL();
         }

@@ -42,8 +42,8 @@ namespace gs {
 struct Tc2Args {
     const float2* W;         // window spectra (PfaCols column order), Nw x L2
     const float2* P;         // template-pair spectra of this angle (PfaCols order), Np x L2
-    const __half2* W16;      // the same in FP16, each window scaled by its s_w (max |.| < 1)
-    const __half2* P16;      // the same in FP16, each pair scaled by its s_p
+    const __half2* W16;      // the same in FP16, row-tile order (k_to_half_tiles), scaled by s_w
+    const __half2* P16;      // the same for the pairs, scaled by s_p
     __half2* R;              // scratch ring, S x L2 half2 (FP16 re, im in 8-column blocks)
     const float* wmax;       // per window max |W|
     const float* pmax;       // per pair max |P|
@@ -280,80 +280,55 @@ __device__ __forceinline__ void tc2_transition(const Tc2Wg& w) {
     }
 }
 
-// Per-thread constants of the row fill: chunk i of warp w covers the column
-// pairs c = 64 (w + 4 i) + 2 lane, c + 1 (12 chunks of 64 columns per row,
-// the last 16 wide, so warp w takes chunks w, w + 4, w + 8); the A1 offsets
-// of both columns (row group n1, K position (n2, re/im)) without the row v,
-// and whether the pair exists.
-struct Tc2FillMap {
-    uint32_t off[6];  // [2 i + column of the pair]
-    uint32_t valid;   // bit i
-    int col[3];       // load offset of chunk i in column pairs (0 for a chunk past the row end)
-};
-template <class C>
-__device__ __forceinline__ Tc2FillMap tc2_fill_map(int wt) {
-    Tc2FillMap f;
-    f.valid = 0u;
-    const int warp = wt >> 5, lane = wt & 31;
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const int c = 64 * (warp + 4 * i) + 2 * lane + q;
-            const int n1 = c / C::N2, n2 = c - n1 * C::N2;
-            f.off[2 * i + q] = (uint32_t)(n2 >> 2) * C::LBO1R + (uint32_t)n1 * 128 + (uint32_t)(n2 & 3) * 4;
-            if (q == 0 && c < C::L) f.valid |= 1u << i;  // L is even: c < L implies c + 1 < L
-        }
-#pragma unroll
-    for (int i = 0; i < 3; ++i) f.col[i] = ((f.valid >> i) & 1u) ? 32 * (warp + 4 * i) + lane : 0;
-    return f;
+// Conjugate product of two FP16 complex numbers (re, im) in half2
+// arithmetic: w conj(p) = (w_re p_re + w_im p_im, w_im p_re - w_re p_im).
+__device__ __forceinline__ uint32_t cmulc_h2(uint32_t wu, uint32_t pu) {
+    const __half2 w = *reinterpret_cast<const __half2*>(&wu);
+    const __half2 p = *reinterpret_cast<const __half2*>(&pu);
+    const __half2 pre = __low2half2(p);                                     // (p_re, p_re)
+    const __half2 pim = __hmul2(__high2half2(p), __floats2half2_rn(1.0f, -1.0f));  // (p_im, -p_im)
+    const __half2 r = __hfma2(__lowhigh2highlow(w), pim, __hmul2(w, pre));
+    return *reinterpret_cast<const uint32_t*>(&r);
 }
 
-// Row tile t of unit u: spectrum rows spectrum_row(8 t + v) of the FP16
-// window and pair spectra (each already scaled to max |.| < 1), their
-// product into A1 (row pass layout: row m = v + 8 n1 of the operand is
-// 8-row group n1, row v in it).  Four rounds of two rows, every load of a
-// round in flight together (8-byte loads of two columns).
+// Row tile t of unit u from the FP16 spectra in tile order (k_to_half_tiles):
+// rows 8 t .. 8 t + 7 hold spectrum rows spectrum_row(8 t + v), each as 16
+// groups n1 of 48 values n2 (45 and three zeros), in A1's K order.  A task
+// is 4 consecutive n2 of one (v, n1): two 16-byte loads, four conjugate
+// products in half2 arithmetic, one 16-byte store at A1's (K group n2 / 4,
+// row m = v + 8 n1).  The K padding comes from the zeros.  Consecutive lanes
+// take consecutive groups: coalesced loads, and LBO1R = 16 mod 128 keeps
+// the stores conflict-free.  Two rounds of six tasks per thread.
 template <class C>
-__device__ __forceinline__ void tc2_row_fill(const Tc2Args& a, int u, int t, const Tc2Wg& w, const Tc2FillMap& fm) {
+__device__ __forceinline__ void tc2_row_fill(const Tc2Args& a, int u, int t, const Tc2Wg& w) {
+    constexpr int G = C::N2P / 4;               // 12 groups of 4 per (v, n1)
+    constexpr int kRow = 16 * C::N2P;           // 768 values per row
+    constexpr int kTasks = C::V * 16 * G;       // 1536
+    constexpr int kRounds = 2;
+    constexpr int kPer = kTasks / 128 / kRounds;  // 6 per round
+    static_assert(kTasks % (128 * kRounds) == 0, "tasks");
     const int2 wp = __ldg(a.unit_wp + u);
-    const int warp = w.wt >> 5, lane = w.wt & 31;
-    const uint2* Wr = reinterpret_cast<const uint2*>(a.W16 + (long long)wp.x * a.L2);
-    const uint2* Pr = reinterpret_cast<const uint2*>(a.P16 + (long long)wp.y * a.L2);
+    const uint4* Wt = reinterpret_cast<const uint4*>(a.W16 + ((long long)wp.x * C::L + 8 * t) * kRow);
+    const uint4* Pt = reinterpret_cast<const uint4*>(a.P16 + ((long long)wp.y * C::L + 8 * t) * kRow);
     const unsigned long long keep = l2_policy_evict_last();
 #pragma unroll 1
-    for (int v0 = 0; v0 < C::V; v0 += 2) {
-        uint2 wv[2][3], pv[2][3];
+    for (int round = 0; round < kRounds; ++round) {
+        uint4 wv[kPer], pv[kPer];
 #pragma unroll
-        for (int r = 0; r < 2; ++r) {
-            const int row = C::Pfa::spectrum_row(8 * t + v0 + r) * (C::L / 2);  // in uint2 (column pairs)
-            // every lane loads (a chunk past the row end re-reads column 0)
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                asm volatile("ld.global.L1::no_allocate.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;"
-                             : "=r"(wv[r][i].x), "=r"(wv[r][i].y) : "l"(Wr + row + fm.col[i]), "l"(keep));
-                pv[r][i] = __ldg(Pr + row + fm.col[i]);
-            }
+        for (int i = 0; i < kPer; ++i) {
+            const int q = w.wt + 128 * (kPer * round + i);   // (v, n1, g), g fastest: uint4 index q
+            asm volatile("ld.global.L1::no_allocate.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+                         : "=r"(wv[i].x), "=r"(wv[i].y), "=r"(wv[i].z), "=r"(wv[i].w) : "l"(Wt + q), "l"(keep));
+            pv[i] = __ldg(Pt + q);
         }
 #pragma unroll
-        for (int r = 0; r < 2; ++r) {
-            const uint32_t dst = w.as + (uint32_t)(v0 + r) * 16;
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int q = 0; q < 2; ++q) {
-                    const uint32_t wq = q ? wv[r][i].y : wv[r][i].x, pq = q ? pv[r][i].y : pv[r][i].x;
-                    const float2 wf = __half22float2(*reinterpret_cast<const __half2*>(&wq));
-                    const float2 pf = __half22float2(*reinterpret_cast<const __half2*>(&pq));
-                    const float2 x = cmulc(wf, pf);
-                    sts32_if(dst + fm.off[2 * i + q], pack_half2(x.x, x.y), (fm.valid >> i) & 1u);
-                }
+        for (int i = 0; i < kPer; ++i) {
+            const int q = w.wt + 128 * (kPer * round + i);
+            const int g = q % G, vn = q / G, n1 = vn & 15, v = vn >> 4;
+            const uint4 x = make_uint4(cmulc_h2(wv[i].x, pv[i].x), cmulc_h2(wv[i].y, pv[i].y),
+                                       cmulc_h2(wv[i].z, pv[i].z), cmulc_h2(wv[i].w, pv[i].w));
+            sts128(w.as + (uint32_t)g * C::LBO1R + (uint32_t)n1 * 128 + (uint32_t)v * 16, x);
         }
-    }
-    // K padding n2 = 45 .. 47 (K group 11, entries 1 .. 3): zero (their B rows are zero too)
-    for (int i = w.wt; i < 128 * 3; i += 128) {
-        const int m = i / 3, n2 = 45 + (i - (i / 3) * 3);
-        sts32(w.as + 11u * C::LBO1R + (uint32_t)(m >> 3) * 128 + (uint32_t)(m & 7) * 16 + (uint32_t)(n2 & 3) * 4, 0u);
     }
 }
 
@@ -366,7 +341,7 @@ __device__ __forceinline__ void tc2_col_fill(const Tc2Args& a, int u, int t, con
     const unsigned long long drop = l2_policy_evict_first();
     constexpr int kChunks = 2 * C::L;  // (row, half)
     constexpr int kPer = 6;            // 16-byte chunks in flight per thread
-    static_assert(kChunks <= 2 * kPer * 128, "two batches");
+    static_assert(kChunks <= 2 * kPer * 128, "two rounds");
     for (int base = 0; base < kChunks; base += kPer * 128) {
     uint4 vals[kPer];
 #pragma unroll
@@ -613,7 +588,6 @@ __global__ void __launch_bounds__(Tc2Cfg<kProducts>::kThreads, 1) k_corr_tc2(Tc2
     w.tmem = *tslot + (uint32_t)w.g * C::tmem_cols;
     w.ish = reinterpret_cast<int*>(sm + C::off_misc + 16) + 4 * w.g;
     const Tc2Masks ymask = tc2_row_masks<C>(w.wt, a.yb0, a.yb1);
-    const Tc2FillMap fmap = tc2_fill_map<C>(w.wt);
     const int total = (a.nu + a.lag) * 2 * C::T;
     // The pipeline leader claims batches of kBatch consecutive items (one
     // atomic per batch), the pipeline processes them in order and the leader
@@ -644,7 +618,7 @@ __global__ void __launch_bounds__(Tc2Cfg<kProducts>::kThreads, 1) k_corr_tc2(Tc2
         const int s = item / (2 * C::T), j = item - s * (2 * C::T);
         if (j < C::T) {
             if (s < a.nu) {
-                tc2_row_fill<C>(a, s, j, w, fmap);
+                tc2_row_fill<C>(a, s, j, w);
                 ok &= tc2_gemm<C, false, false>(w, sm, phase, a.error);
                 tc2_transition<C>(w);
                 ok &= tc2_gemm<C, true, false>(w, sm, phase, a.error, tc2_row_dep<C>(a, s));
@@ -689,15 +663,22 @@ __global__ void __launch_bounds__(Tc2Cfg<kProducts>::kThreads, 1) k_corr_tc2(Tc2
     if ((threadIdx.x >> 5) == 0) tc::tmem_dealloc(*tslot, 512);
 }
 
-// FP16 copy of `count` images of l2 complex values, image i scaled by the
-// exact power of two tc2_scale1(maxabs[i]).
-__global__ void k_to_half_scaled(const float2* __restrict__ z, long long l2, const float* __restrict__ maxabs,
-                                 __half2* __restrict__ out) {
+// FP16 copy of `count` window or pair spectra (PfaCols column order, natural
+// row order) in the all-tensor-core row tiles' order: image i scaled by the
+// exact power of two tc2_scale1(maxabs[i]); row r of the copy holds spectrum
+// row spectrum_row(r) as 16 groups n1 of 48 values (physical columns
+// 45 n1 .. 45 n1 + 44, then three zeros).
+__global__ void k_to_half_tiles(const float2* __restrict__ z, const float* __restrict__ maxabs,
+                                __half2* __restrict__ out) {
+    using F = CorrCfg<45, 16>;
+    constexpr int L = 720, kRow = 16 * 48;
     const float s = tc2_scale1(__ldg(maxabs + blockIdx.y));
-    const float2* img = z + (long long)blockIdx.y * l2;
-    __half2* o = out + (long long)blockIdx.y * l2;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < l2; i += (long long)gridDim.x * blockDim.x) {
-        const float2 v = img[i];
+    const float2* img = z + (long long)blockIdx.y * L * L;
+    __half2* o = out + (long long)blockIdx.y * L * kRow;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L * kRow; i += gridDim.x * blockDim.x) {
+        const int r = i / kRow, rest = i - r * kRow, n1 = rest / 48, n2 = rest - n1 * 48;
+        float2 v = make_float2(0.0f, 0.0f);
+        if (n2 < 45) v = img[(long long)F::spectrum_row(r) * L + 45 * n1 + n2];
         o[i] = __floats2half2_rn(v.x * s, v.y * s);
     }
 }
