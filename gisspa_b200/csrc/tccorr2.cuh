@@ -265,19 +265,26 @@ template <class C>
 __device__ __forceinline__ void tc2_transition(const Tc2Wg& w) {
     const int m = w.wt, v = m & 7, n1 = m >> 3;
     const uint32_t lane_base = w.tmem + ((uint32_t)(32 * (w.wt >> 5)) << 16);
-    uint32_t r[32];
     const uint32_t dst = w.as + (uint32_t)(n1 >> 2) * C::LBO2 + (uint32_t)v * 16 + (uint32_t)(n1 & 3) * 4;
-#pragma unroll 1
-    for (int q = 0; q < 3; ++q) {
-        tc::tmem_ld32(lane_base + 32 * q, r);
-        tc::tmem_ld_wait();
+    // A1 (aliased by A2) is no longer read: the stage-1 MMAs completed.  The
+    // next 32 columns are loaded while the current ones are converted and
+    // stored (tcgen05.wait::ld waits for every load issued before it).
+    uint32_t r0[32], r1[32];
+    tc::tmem_ld32(lane_base, r0);
+    tc::tmem_ld_wait();
+    tc::tmem_ld32(lane_base + 32, r1);
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
-            // A1 (aliased by A2) is no longer read: the stage-1 MMAs completed
-            const int k2 = 16 * q + i;
-            sts32(dst + (uint32_t)k2 * 128, pack_half2(__uint_as_float(r[2 * i]), __uint_as_float(r[2 * i + 1])));
-        }
-    }
+    for (int i = 0; i < 16; ++i)
+        sts32(dst + (uint32_t)i * 128, pack_half2(__uint_as_float(r0[2 * i]), __uint_as_float(r0[2 * i + 1])));
+    tc::tmem_ld_wait();
+    tc::tmem_ld32(lane_base + 64, r0);
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+        sts32(dst + (uint32_t)(16 + i) * 128, pack_half2(__uint_as_float(r1[2 * i]), __uint_as_float(r1[2 * i + 1])));
+    tc::tmem_ld_wait();
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+        sts32(dst + (uint32_t)(32 + i) * 128, pack_half2(__uint_as_float(r0[2 * i]), __uint_as_float(r0[2 * i + 1])));
 }
 
 // Conjugate product of two FP16 complex numbers (re, im) in half2
@@ -376,13 +383,11 @@ __device__ __forceinline__ void tc2_row_out(const Tc2Args& a, int u, int t, cons
     const uint32_t lane_base = w.tmem + ((uint32_t)(32 * (w.wt >> 5)) << 16);
     const int v = w.wt & 7;
     const unsigned long long keep = l2_policy_evict_last();
-#pragma unroll 1
-    for (int ti = 0; ti < C::MT2; ++ti) {
-        uint32_t r[32];
-        tc::tmem_ld32(lane_base + 32 * ti, r);
-        tc::tmem_ld_wait();
+    // one stage-2 tile's 16 k1 values of row (k2, v): two 8-column blocks
+    // [re x 8][im x 8] of FP16 map row 8 t + v
+    auto put = [&](const uint32_t* r, int ti) {
         const int k2 = 16 * ti + (w.wt >> 3);
-        if (k2 >= C::N2) continue;
+        if (k2 >= C::N2) return;
         uint32_t o[16];
 #pragma unroll
         for (int blk = 0; blk < 2; ++blk)
@@ -394,12 +399,22 @@ __device__ __forceinline__ void tc2_row_out(const Tc2Args& a, int u, int t, cons
             }
         uint4* dst = reinterpret_cast<uint4*>(Rs + (long long)(8 * t + v) * C::L + 16 * k2);
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const uint4 val = make_uint4(o[4 * i], o[4 * i + 1], o[4 * i + 2], o[4 * i + 3]);
+        for (int i = 0; i < 4; ++i)
             asm volatile("st.global.L1::no_allocate.L2::cache_hint.v4.u32 [%0], {%1, %2, %3, %4}, %5;"
-                         ::"l"(dst + i), "r"(val.x), "r"(val.y), "r"(val.z), "r"(val.w), "l"(keep) : "memory");
-        }
-    }
+                         ::"l"(dst + i), "r"(o[4 * i]), "r"(o[4 * i + 1]), "r"(o[4 * i + 2]), "r"(o[4 * i + 3]),
+                         "l"(keep) : "memory");
+    };
+    // the next tile's columns are loaded while the current ones are stored
+    uint32_t r0[32], r1[32];
+    tc::tmem_ld32(lane_base, r0);
+    tc::tmem_ld_wait();
+    tc::tmem_ld32(lane_base + 32, r1);
+    put(r0, 0);
+    tc::tmem_ld_wait();
+    tc::tmem_ld32(lane_base + 64, r0);
+    put(r1, 1);
+    tc::tmem_ld_wait();
+    put(r0, 2);
 }
 
 // Border mask of the map rows this thread's stage-2 lanes hold: bit k1 of
@@ -442,19 +457,15 @@ __device__ __forceinline__ void tc2_col_out(const Tc2Args& a, int u, int t, cons
     const bool xin = (unsigned)(x - a.yb0) <= (unsigned)(a.yb1 - a.yb0);  // column in the border
     float b1 = 0.0f, b2 = 0.0f, s2a = 0.0f, s2b = 0.0f;
     int k1a = -1, k1b = -1, tia = 0, tib = 0;
-    // the tile loop stays rolled: one 32-register array is live at a time
-#pragma unroll 1
-    for (int ti = 0; ti < C::MT2; ++ti) {
-        uint32_t r[32];
-        tc::tmem_ld32(lane_base + 32 * ti, r);
-        tc::tmem_ld_wait();
-        // rows k2 >= 45 hold zeros and no bits
-        const uint32_t bits = xin ? 0u : (ti == 0 ? mb.m[0] : ti == 1 ? mb.m[1] : mb.m[2]);
+    // eight k1 values (half `hf` of tile ti); rows k2 >= 45 hold zeros and no bits
+    auto take = [&](const float* r, int ti, int hf) {
+        const uint32_t bits = xin ? 0u : (mb.m[ti] >> (8 * hf));
         const float b1_0 = b1, b2_0 = b2;
 #pragma unroll
-        for (int k1 = 0; k1 < 16; ++k1) {
-            const float v1 = __uint_as_float(r[2 * k1]), v2 = __uint_as_float(r[2 * k1 + 1]);
-            const bool in = (bits >> k1) & 1u;
+        for (int kk = 0; kk < 8; ++kk) {
+            const int k1 = 8 * hf + kk;
+            const float v1 = r[2 * kk], v2 = r[2 * kk + 1];
+            const bool in = (bits >> kk) & 1u;
             const bool g1 = in && v1 > b1, g2 = in && v2 > b2;
             b1 = g1 ? v1 : b1;
             k1a = g1 ? k1 : k1a;
@@ -463,10 +474,31 @@ __device__ __forceinline__ void tc2_col_out(const Tc2Args& a, int u, int t, cons
             s2a = fmaf(v1, v1, s2a);
             s2b = fmaf(v2, v2, s2b);
         }
-        // the maximum only grows strictly: it changed iff it now lies in this tile
+        // the maximum only grows strictly: it changed iff it now lies here
         tia = b1 != b1_0 ? ti : tia;
         tib = b2 != b2_0 ? ti : tib;
-    }
+    };
+    // 16-column halves, the next one loaded while the current one is reduced
+    // (tcgen05.wait::ld waits for every load issued before it)
+    float ra[16], rb[16];
+    tc::tmem_ld16(lane_base, ra);
+    tc::tmem_ld_wait();
+    tc::tmem_ld16(lane_base + 16, rb);
+    take(ra, 0, 0);
+    tc::tmem_ld_wait();
+    tc::tmem_ld16(lane_base + 32, ra);
+    take(rb, 0, 1);
+    tc::tmem_ld_wait();
+    tc::tmem_ld16(lane_base + 48, rb);
+    take(ra, 1, 0);
+    tc::tmem_ld_wait();
+    tc::tmem_ld16(lane_base + 64, ra);
+    take(rb, 1, 1);
+    tc::tmem_ld_wait();
+    tc::tmem_ld16(lane_base + 80, rb);
+    take(ra, 2, 0);
+    tc::tmem_ld_wait();
+    take(rb, 2, 1);
     const int X = x + h < L ? x + h : x - h;
     auto key_of = [&](float b, int k1, int ti) -> unsigned long long {
         if (k1 < 0) return 0ull;

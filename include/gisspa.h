@@ -311,7 +311,10 @@ int gs_set_kernel_timing(struct gs_ctx* ctx, int enable);
 #define GS_OPT_WINDOW_BLOCK 3
 /* GS_OPT_CORR_SLOTS / GS_OPT_CORR_LAG: scratch maps in the persistent
  * launch's ring (default 16) and how many units after its row tiles a unit's
- * column tiles are queued (default 6); slots must exceed lag. */
+ * column tiles are queued (default 6); slots must exceed lag.  The
+ * all-tensor-core modes keep more items in flight and default to 24 slots and
+ * a lag of 12 unless either option was set; they need lag >= 1 and
+ * slots >= lag + 2 (GS_ERR_UNSUPPORTED otherwise). */
 #define GS_OPT_CORR_SLOTS 4
 #define GS_OPT_CORR_LAG 5
 /* GS_OPT_CORR_CTAS: resident CTAs per SM of the persistent launch (0 = as
