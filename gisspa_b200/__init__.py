@@ -392,6 +392,17 @@ class Context:
         self._check(self._lib.gs_get_tuning(self._h, t, 5), "gs_get_tuning")
         return tuple(t[:])
 
+    def set_angles_per_launch(self, angles: int) -> None:
+        """In-plane angles per persistent correlation launch (GS_OPT_ANGLES_PER_LAUNCH;
+        0 = chosen from the unit count)."""
+        self._check(self._lib.gs_set_option(self._h, 10, int(angles)), "gs_set_option")
+
+    def angles_per_launch(self) -> int:
+        """In-plane angles per persistent launch of the last search."""
+        t = (C.c_int * 6)()
+        self._check(self._lib.gs_get_tuning(self._h, t, 6), "gs_get_tuning")
+        return int(t[5])
+
     def set_corr_tile(self, vectors: int) -> None:
         """Tile width of the FP32 persistent kernel (16 or 8 vectors)."""
         self._check(self._lib.gs_set_option(self._h, 9, int(vectors)), "gs_set_option")

@@ -53,19 +53,29 @@ namespace gs {
 
 struct CorrArgs {
     const float2* W;         // window spectra, Nw x L2
-    const float2* P;         // template-pair spectra of this angle, Np x L2
+    const float2* P;         // template-pair spectra of the launch's angles, (angles x pairs) x L2
     float2* R;               // scratch ring, S x L2
-    const int2* unit_wp;     // unit -> (window, pair)
+    const int2* unit_wp;     // unit -> (window, angle x pairs + pair)
     int* done_rows;          // per unit, row tiles finished
     int* done_cols;          // per unit, column tiles finished
     UnitAcc* acc;            // per unit, 2 templates
-    UnitOut* out;            // this angle's results, index w * ntmpl + J
+    UnitOut* out;            // results, index angle * out_stride + w * ntmpl + J
     int* next_item;          // claim counter
     int* error;              // set when a bounded wait gives up
     int nu, ntmpl, S, lag;
     long long L2;
     int yb0, yb1;            // border interval of unshifted indices (both axes)
+    int pairs;               // template pairs per angle
+    long long out_stride;    // results per angle (windows x templates)
 };
+
+// Results slot of template q (0, 1) of pair index y = angle x pairs + pair
+// for window w, or -1 when the pair has no second template (odd count).
+__device__ __forceinline__ long long unit_out_index(int y, int q, int w, int pairs, int ntmpl,
+                                                    long long out_stride) {
+    const int an = y / pairs, J = 2 * (y - an * pairs) + q;
+    return J < ntmpl ? an * out_stride + (long long)w * ntmpl + J : -1;
+}
 
 __device__ __forceinline__ int ld_acquire_gpu(const int* p) {
     int v;
@@ -423,12 +433,12 @@ __device__ __forceinline__ void corr_publish(const CorrArgs& a, int item) {
     const double sums[2] = {sg * l2 * ((double)w0.x * p0.x + (double)w0.y * p0.y),
                             sg * l2 * ((double)w0.y * p0.x - (double)w0.x * p0.y)};
     for (int q = 0; q < 2; ++q) {
-        const int J = 2 * wp.y + q;
-        if (J >= a.ntmpl) break;
+        const long long o = unit_out_index(wp.y, q, wp.x, a.pairs, a.ntmpl, a.out_stride);
+        if (o < 0) break;
         UnitAcc v;
         v.key = __ldcg(&ac[q].key);
         v.s2 = __ldcg(&ac[q].s2);
-        a.out[(long long)wp.x * a.ntmpl + J] = unit_score(v, sums[q], F::L);
+        a.out[o] = unit_score(v, sums[q], F::L);
     }
 }
 

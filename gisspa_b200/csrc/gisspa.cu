@@ -86,11 +86,14 @@ struct gs_ctx {
     bool use_graph = false;            // capture the angle loop as one CUDA graph
     bool autotune = false;             // tune the persistent kernels' scheduling on first use
     std::map<long long, struct CorrTuningSaved> tuned;
-    int last_tuning[5] = {0, 0, 0, 0, 0};
+    int angles_per_launch = 0;         // in-plane angles per persistent launch (0 = from the unit count)
+    std::map<long long, int> tuned_angles;  // the autotuner's angles per launch, same key as `tuned`
+    int last_tuning[6] = {0, 0, 0, 0, 0, 0};
     unsigned long long graph_kernel_launches = 0;
     DBuf unit_wp, dep_counters, pacc, flags;
     DBuf tc2_wmax, tc2_pmax;  // per window / per pair max |spectrum| (all-tensor-core path)
     DBuf tc2_w16, tc2_p16;    // their FP16 copies, scaled by powers of two
+    DBuf rot_cs;              // (cos, sin) of every in-plane angle of the search
     // off-grid refinement (refine.cuh): per-pick chunk buffers
     DBuf rf_pk, rf_acc, rf_B, rf_F1, rf_T, rf_TM, rf_F, rf_G, rf_TB, rf_mask;
     std::vector<cudaEvent_t> kev;  // pool of events for per-kernel timing
@@ -402,31 +405,43 @@ unsigned blocks_for(long long n, int threads, unsigned cap = 1u << 30) {
 // with each rotated, masked template mean/variance normalised.
 // pfa: store the spectra in the PfaCols column order of the prime-factor
 // correlation kernel (window 720) instead of natural order.
-static int pair_spectra(gs_ctx* ctx, float e, float2* TS, bool pfa = false) {
+// (cos, sin) of in-plane angle e (degrees) as the rotation takes them.
+static float2 rotation_cs(float e) {
+    const double ang = (double)e * kPiRef / 180.0;
+    return make_float2((float)cos(ang), (float)sin(ang));
+}
+// The spectra of `nang` consecutive angles in one pass (angle z's at
+// TS + z Np l^2; pstats and coef hold nang angles): cs = their (cos, sin) on
+// the device, or nullptr for the single angle e.
+static int pair_spectra_n(gs_ctx* ctx, float e, const float2* cs, int nang, float2* TS, bool pfa) {
     const int l = ctx->l, N = ctx->ntmpl, Np = (N + 1) / 2;
     const long long l2 = (long long)l * l;
-    const double ang = (double)e * kPiRef / 180.0;
-    const float cose = (float)cos(ang), sine = (float)sin(ang);
-    CK(cudaMemsetAsync(ctx->pstats.p, 0, sizeof(double) * 2 * N, ctx->stream));
-    dim3 g(blocks_for(l2, 256, 32), Np);
-    k_pair_rotate<<<g, 256, 0, ctx->stream>>>(P<float>(ctx->tmpl), N, l, cose, sine, ctx->p.d_m, TS,
+    const float2 c = rotation_cs(e);
+    const int nimg = Np * nang;
+    CK(cudaMemsetAsync(ctx->pstats.p, 0, sizeof(double) * 2 * N * nang, ctx->stream));
+    dim3 g(blocks_for(l2, 256, 32), Np, nang);
+    k_pair_rotate<<<g, 256, 0, ctx->stream>>>(P<float>(ctx->tmpl), N, l, c.x, c.y, cs, ctx->p.d_m, TS,
                                               P<double>(ctx->pstats));
     ++ctx->counters.kernel_launches;
-    k_pair_coef<<<blocks_for(Np, 128), 128, 0, ctx->stream>>>(P<double>(ctx->pstats), N, l, P<float4>(ctx->coef));
+    k_pair_coef<<<blocks_for(nimg, 128), 128, 0, ctx->stream>>>(P<double>(ctx->pstats), N, l,
+                                                                P<float4>(ctx->coef), nang);
     ++ctx->counters.kernel_launches;
     CKL();
     if (fast_ok(ctx, l)) {
         const F16PairNorm rows{TS, P<float4>(ctx->coef), l, l2};
         if (pfa)
-            TRY(run_fast<false, false>(ctx, l, Np, F16PairNormPfa{rows, PfaCols::make(l)}));
+            TRY(run_fast<false, false>(ctx, l, nimg, F16PairNormPfa{rows, PfaCols::make(l)}));
         else
-            TRY(run_fast<false, false>(ctx, l, Np, rows));
-        TRY(run_fast<false, true>(ctx, l, Np, F16Complex<true>{TS, l, l2, (float)(1.0 / (double)l2)}));
+            TRY(run_fast<false, false>(ctx, l, nimg, rows));
+        TRY(run_fast<false, true>(ctx, l, nimg, F16Complex<true>{TS, l, l2, (float)(1.0 / (double)l2)}));
     } else {
-        TRY(run_fft<false>(ctx, l, rows_of(l, l), Np, IoPairNorm{TS, P<float4>(ctx->coef), l2}));
-        TRY(run_fft<false>(ctx, l, cols_of(l, l), Np, IoComplex{TS, (float)(1.0 / (double)l2)}));
+        TRY(run_fft<false>(ctx, l, rows_of(l, l), nimg, IoPairNorm{TS, P<float4>(ctx->coef), l2}));
+        TRY(run_fft<false>(ctx, l, cols_of(l, l), nimg, IoComplex{TS, (float)(1.0 / (double)l2)}));
     }
     return GS_OK;
+}
+static int pair_spectra(gs_ctx* ctx, float e, float2* TS, bool pfa = false) {
+    return pair_spectra_n(ctx, e, nullptr, 1, TS, pfa);
 }
 
 // Row pass of the correlation of window spectrum Ww with the Np pair spectra
@@ -859,7 +874,8 @@ int gs_ctx_destroy(gs_ctx* ctx) {
                     &ctx->coef, &ctx->acc, &ctx->units, &ctx->picks, &ctx->count, &ctx->unit_wp,
                     &ctx->dep_counters, &ctx->pacc, &ctx->flags, &ctx->tbase, &ctx->rf_pk, &ctx->rf_acc,
                     &ctx->rf_B, &ctx->rf_F1, &ctx->rf_T, &ctx->rf_TM, &ctx->rf_F, &ctx->rf_G, &ctx->rf_TB,
-                    &ctx->rf_mask};
+                    &ctx->rf_mask, &ctx->pix_keys, &ctx->pix_pairs, &ctx->pix_R, &ctx->tc2_wmax,
+                    &ctx->tc2_pmax, &ctx->tc2_w16, &ctx->tc2_p16, &ctx->rot_cs};
     for (DBuf* b : bufs) free_buf(*b);
     for (cudaEvent_t e : ctx->kev) cudaEventDestroy(e);
     cudaStreamDestroy(ctx->stream);
@@ -1124,14 +1140,17 @@ struct CorrTuning {
     int slots, lag, window_block, ctas, tile;
 };
 
-// Unit order: blocks of window_block windows; inside a block, pair-major.
-static int upload_unit_order(gs_ctx* ctx, int NW, int Np, int wbk, int limit) {
+// Unit order: angle-major over the launch's `angles` angles (pair index
+// angle x Np + pair); within an angle blocks of window_block windows, inside
+// a block pair-major.
+static int upload_unit_order(gs_ctx* ctx, int NW, int Np, int wbk, int limit, int angles = 1) {
     std::vector<int2> wp;
-    wp.reserve((size_t)NW * Np);
+    wp.reserve((size_t)NW * Np * angles);
     wbk = std::max(1, wbk);
-    for (int w0 = 0; w0 < NW; w0 += wbk)
-        for (int pp = 0; pp < Np; ++pp)
-            for (int w = w0; w < std::min(NW, w0 + wbk); ++w) wp.push_back(make_int2(w, pp));
+    for (int an = 0; an < angles; ++an)
+        for (int w0 = 0; w0 < NW; w0 += wbk)
+            for (int pp = 0; pp < Np; ++pp)
+                for (int w = w0; w < std::min(NW, w0 + wbk); ++w) wp.push_back(make_int2(w, an * Np + pp));
     const size_t n = std::min(wp.size(), (size_t)limit);
     TRY(ensure(ctx, ctx->unit_wp, sizeof(int2) * std::max<size_t>(1, wp.size())));
     CK(cudaMemcpyAsync(ctx->unit_wp.p, wp.data(), sizeof(int2) * n, cudaMemcpyHostToDevice, ctx->stream));
@@ -1140,9 +1159,11 @@ static int upload_unit_order(gs_ctx* ctx, int NW, int Np, int wbk, int limit) {
     return GS_OK;
 }
 
-// One persistent correlation launch over the first nu units (angle ai's
-// template-pair spectra already in TS), results to out.
-static int corr_launch(gs_ctx* ctx, const float2* W, const float2* TS, int nu, const CorrTuning& t, UnitOut* out) {
+// One persistent correlation launch over the first nu units (the template-pair
+// spectra of the launch's angles already in TS, angle after angle), results
+// to out, out_stride results per angle.
+static int corr_launch(gs_ctx* ctx, const float2* W, const float2* TS, int nu, const CorrTuning& t, UnitOut* out,
+                       long long out_stride = 0) {
     const int l = ctx->l;
     const long long l2 = (long long)l * l;
     int* cnt = P<int>(ctx->dep_counters);
@@ -1157,6 +1178,8 @@ static int corr_launch(gs_ctx* ctx, const float2* W, const float2* TS, int nu, c
     ca.next_item = cnt + 2 * (size_t)nu;
     ca.error = P<int>(ctx->flags);
     ca.nu = nu; ca.ntmpl = ctx->ntmpl; ca.S = t.slots; ca.lag = t.lag; ca.L2 = l2;
+    ca.pairs = (ctx->ntmpl + 1) / 2;
+    ca.out_stride = out_stride;
     // border interval of unshifted indices: X = (x + l/2) mod l is masked
     // when X < d_m/4 or X > l - d_m/4 (GPU_func.cu:681)
     {
@@ -1187,6 +1210,7 @@ static int corr_launch(gs_ctx* ctx, const float2* W, const float2* TS, int nu, c
         a.acc = ca.acc; a.out = ca.out; a.next_item = ca.next_item; a.error = ca.error;
         a.nu = ca.nu; a.ntmpl = ca.ntmpl; a.S = ca.S; a.lag = ca.lag; a.L2 = ca.L2;
         a.yb0 = ca.yb0; a.yb1 = ca.yb1;
+        a.pairs = ca.pairs; a.out_stride = ca.out_stride;
         return ctx->p.precision == GS_PREC_TC_FULL ? launch_corr_tc2_p<2>(ctx, a) : launch_corr_tc2_p<1>(ctx, a);
     }
     return launch_corr_tc(ctx, l, ctx->p.precision == GS_PREC_TC_BF16, ca);
@@ -1286,11 +1310,41 @@ static int correlate_all(gs_ctx* ctx, float2* W, int NW, const std::vector<float
         return set_err(ctx, GS_ERR_UNSUPPORTED,
                        "tensor-core precision needs window 512, 720 or 768 and the persistent path (window %d)", l);
     const int nu = Np * NW;
-    if ((long long)(nu + 64) * 2 * (l / 8) >= (1ll << 31))
+    // item indices of one launch (2 x l/8 tiles per unit) must fit an int
+    auto units_fit = [&](long long n) { return (n + 64) * 2 * (l / 8) < (1ll << 31); };
+    if (!units_fit(nu))
         return set_err(ctx, GS_ERR_UNSUPPORTED, "too many (window, template pair) units in one search (%d)", nu);
-    TRY(ensure(ctx, ctx->tspec, sizeof(float2) * l2 * Np));
-    TRY(ensure(ctx, ctx->pstats, sizeof(double) * 2 * N));
-    TRY(ensure(ctx, ctx->coef, sizeof(float4) * Np));
+    // In-plane angles per persistent launch: by default enough angles for
+    // about kUnitsPerLaunch units (a launch's ramp-up and drain, and the
+    // per-launch overhead, then weigh little against its work), with the
+    // pair spectra of all of them within kAngleBudget bytes; the option
+    // overrides the count, the item-index limit still applies.
+    constexpr long long kUnitsPerLaunch = 16384;
+    constexpr double kAngleBudget = 8.0 * (1ull << 30);
+    const double angle_bytes = (double)sizeof(float2) * l2 * Np +
+                               (tc2 ? (double)sizeof(__half2) * l * 768 * Np + sizeof(float) * Np : 0.0);
+    int A = 1;
+    if (persistent) {
+        if (ctx->angles_per_launch > 0) {
+            A = ctx->angles_per_launch;
+        } else {
+            A = (int)std::max(1ll, kUnitsPerLaunch / nu);
+            A = (int)std::min<double>(A, std::max(1.0, std::floor(kAngleBudget / angle_bytes)));
+        }
+        A = std::max(1, std::min(A, na));
+        while (A > 1 && !units_fit((long long)A * nu)) --A;
+    }
+    TRY(ensure(ctx, ctx->tspec, sizeof(float2) * l2 * Np * A));
+    TRY(ensure(ctx, ctx->pstats, sizeof(double) * 2 * N * A));
+    TRY(ensure(ctx, ctx->coef, sizeof(float4) * Np * A));
+    // every angle's (cos, sin) on the device, for the pair spectra of a group
+    // of angles in one pass (uploaded before any capture)
+    {
+        std::vector<float2> cs(na);
+        for (int i = 0; i < na; ++i) cs[i] = rotation_cs(angles[i]);
+        TRY(ensure(ctx, ctx->rot_cs, sizeof(float2) * std::max(1, na)));
+        CK(cudaMemcpy(ctx->rot_cs.p, cs.data(), sizeof(float2) * na, cudaMemcpyHostToDevice));
+    }
     TRY(ensure(ctx, ctx->acc, sizeof(UnitAcc) * N));
     TRY(ensure(ctx, ctx->units, sizeof(UnitOut) * std::max<long long>(1, total_units)));
     float2* TS = P<float2>(ctx->tspec);
@@ -1329,10 +1383,10 @@ static int correlate_all(gs_ctx* ctx, float2* W, int NW, const std::vector<float
     if (tc2) {
         // per-window max |W| for the FP16 scaling of each unit
         TRY(ensure(ctx, ctx->tc2_wmax, sizeof(float) * NW));
-        TRY(ensure(ctx, ctx->tc2_pmax, sizeof(float) * Np));
+        TRY(ensure(ctx, ctx->tc2_pmax, sizeof(float) * Np * A));
         // FP16 copies in the row tiles' order: l rows of 16 x 48 values
         TRY(ensure(ctx, ctx->tc2_w16, sizeof(__half2) * (size_t)l * 768 * NW));
-        TRY(ensure(ctx, ctx->tc2_p16, sizeof(__half2) * (size_t)l * 768 * Np));
+        TRY(ensure(ctx, ctx->tc2_p16, sizeof(__half2) * (size_t)l * 768 * Np * A));
         CK(cudaMemsetAsync(ctx->tc2_wmax.p, 0, sizeof(float) * NW, ctx->stream));
         k_max_abs<<<dim3(64, NW), 256, 0, ctx->stream>>>(W, l2, P<float>(ctx->tc2_wmax));
         k_to_half_tiles<<<dim3(64, NW), 256, 0, ctx->stream>>>(W, P<float>(ctx->tc2_wmax), P<__half2>(ctx->tc2_w16));
@@ -1340,8 +1394,8 @@ static int correlate_all(gs_ctx* ctx, float2* W, int NW, const std::vector<float
         CKL();
     }
     if (persistent) {
-        TRY(ensure(ctx, ctx->dep_counters, sizeof(int) * (2 * (size_t)nu + 4)));
-        TRY(ensure(ctx, ctx->pacc, sizeof(UnitAcc) * 2 * (size_t)nu));
+        TRY(ensure(ctx, ctx->dep_counters, sizeof(int) * (2 * (size_t)nu * A + 4)));
+        TRY(ensure(ctx, ctx->pacc, sizeof(UnitAcc) * 2 * (size_t)nu * A));
         TRY(ensure(ctx, ctx->flags, sizeof(int) * 4));
         CK(cudaMemsetAsync(ctx->flags.p, 0, sizeof(int) * 4, ctx->stream));
         if (ctx->autotune) {
@@ -1357,7 +1411,8 @@ static int correlate_all(gs_ctx* ctx, float2* W, int NW, const std::vector<float
             }
             TRY(autotune(ctx, W, TS, NW, &tune));
         }
-        TRY(upload_unit_order(ctx, NW, Np, tune.window_block, nu));
+        // angle-major: a launch of fewer angles takes a prefix of this order
+        TRY(upload_unit_order(ctx, NW, Np, tune.window_block, nu * A, A));
         TRY(ensure(ctx, ctx->scratch, sizeof(float2) * l2 * tune.slots));
     } else {
         TRY(ensure(ctx, ctx->scratch, sizeof(float2) * l2 * Np));
@@ -1388,25 +1443,39 @@ static int correlate_all(gs_ctx* ctx, float2* W, int NW, const std::vector<float
     float k1ms = 0, k2ms = 0;
     long long k1n = 0, k2n = 0;
 
-    // the work of one angle, enqueued on the context's stream
-    auto enqueue_angle = [&](int ai, bool rec) -> int {
+    // the work of angles a0 .. a0 + ag - 1 (ag = 1 without the persistent
+    // kernel), enqueued on the context's stream: their pair spectra one
+    // after the other in TS, then one correlation launch over all their units
+    auto enqueue_group = [&](int a0, int ag, bool rec) -> int {
         if (rec) CK(cudaEventRecord(ea, ctx->stream));
-        TRY(pair_spectra(ctx, angles[ai], TS, pfa));
-        if (tc2) {
-            CK(cudaMemsetAsync(ctx->tc2_pmax.p, 0, sizeof(float) * Np, ctx->stream));
-            k_max_abs<<<dim3(64, Np), 256, 0, ctx->stream>>>(TS, l2, P<float>(ctx->tc2_pmax));
-            k_to_half_tiles<<<dim3(64, Np), 256, 0, ctx->stream>>>(TS, P<float>(ctx->tc2_pmax),
-                                                                  P<__half2>(ctx->tc2_p16));
-            ctx->counters.kernel_launches += 2;
-            CKL();
+        // pair spectra of the group, in passes of at most kImgs images
+        constexpr int kImgs = 32768;
+        const int per = std::max(1, kImgs / Np);
+        for (int k = 0; k < ag; k += per) {
+            const int n = std::min(per, ag - k);
+            TRY(pair_spectra_n(ctx, angles[a0 + k], P<float2>(ctx->rot_cs) + a0 + k, n,
+                               TS + (size_t)k * Np * l2, pfa));
+        }
+        for (int k = 0; k < ag; ++k) {
+            float2* TSk = TS + (size_t)k * Np * l2;
+            if (tc2) {
+                float* pm = P<float>(ctx->tc2_pmax) + (size_t)k * Np;
+                CK(cudaMemsetAsync(pm, 0, sizeof(float) * Np, ctx->stream));
+                k_max_abs<<<dim3(64, Np), 256, 0, ctx->stream>>>(TSk, l2, pm);
+                k_to_half_tiles<<<dim3(64, Np), 256, 0, ctx->stream>>>(
+                    TSk, pm, P<__half2>(ctx->tc2_p16) + (size_t)k * Np * l * 768);
+                ctx->counters.kernel_launches += 2;
+                CKL();
+            }
         }
         if (rec) CK(cudaEventRecord(eb, ctx->stream));
         if (persistent) {
             if (timing) CK(cudaEventRecord(ctx->kev[0], ctx->stream));
-            TRY(corr_launch(ctx, W, TS, nu, tune, units + (size_t)ai * NW * N));
+            TRY(corr_launch(ctx, W, TS, nu * ag, tune, units + (size_t)a0 * NW * N, (long long)NW * N));
             if (timing) CK(cudaEventRecord(ctx->kev[1], ctx->stream));
             return GS_OK;
         }
+        const int ai = a0;
         for (int w = 0; w < NW; ++w) {
             CK(cudaMemsetAsync(acc, 0, sizeof(UnitAcc) * N, ctx->stream));
             const bool fast = fast_ok(ctx, l);
@@ -1433,6 +1502,40 @@ static int correlate_all(gs_ctx* ctx, float2* W, int NW, const std::vector<float
         return GS_OK;
     };
 
+    // Autotuner, angles per launch (when the default groups angles): each
+    // candidate's first group (pair spectra and correlation of angles
+    // 0 .. A - 1) timed once after one warm-up group, time per angle
+    // compared; the choice is cached with the scheduling.
+    if (persistent && ctx->autotune && ctx->angles_per_launch == 0 && A > 1) {
+        const long long key = (((long long)l * 1000003 + N) * 1000003 + NW) * 4 + p.precision;
+        auto it = ctx->tuned_angles.find(key);
+        if (it != ctx->tuned_angles.end()) {
+            A = std::max(1, std::min(A, it->second));
+        } else {
+            std::vector<int> cand = {1, std::max(1, A / 4), std::max(1, A / 2), A};
+            cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+            TRY(enqueue_group(0, cand[0], false));  // warm-up
+            float best = 0.0f;
+            int best_a = A;
+            for (int c : cand) {
+                CK(cudaEventRecord(ea, ctx->stream));
+                TRY(enqueue_group(0, c, false));
+                CK(cudaEventRecord(ec, ctx->stream));
+                CK(cudaEventSynchronize(ec));
+                float ms = 0.0f;
+                CK(cudaEventElapsedTime(&ms, ea, ec));
+                const float per = ms / (float)c;
+                if (c == cand[0] || per < best) {
+                    best = per;
+                    best_a = c;
+                }
+            }
+            ctx->tuned_angles[key] = best_a;
+            A = best_a;
+        }
+    }
+    ctx->last_tuning[5] = A;
+
     if (ctx->use_graph) {
         // the whole angle loop as one CUDA graph: captured once, launched once
         cudaGraph_t graph = nullptr;
@@ -1440,7 +1543,7 @@ static int correlate_all(gs_ctx* ctx, float2* W, int NW, const std::vector<float
         const unsigned long long launches0 = ctx->counters.kernel_launches;
         CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
         int st = GS_OK;
-        for (int ai = 0; ai < na && st == GS_OK; ++ai) st = enqueue_angle(ai, false);
+        for (int ai = 0; ai < na && st == GS_OK; ai += A) st = enqueue_group(ai, std::min(A, na - ai), false);
         const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
         if (st != GS_OK) {
             if (graph) cudaGraphDestroy(graph);
@@ -1458,8 +1561,8 @@ static int correlate_all(gs_ctx* ctx, float2* W, int NW, const std::vector<float
         cudaEventElapsedTime(&t, eb, ec);
         *t_corr += t;
     } else {
-        for (int ai = 0; ai < na; ++ai) {
-            TRY(enqueue_angle(ai, true));
+        for (int ai = 0; ai < na; ai += A) {
+            TRY(enqueue_group(ai, std::min(A, na - ai), true));
             CK(cudaEventRecord(ec, ctx->stream));
             CK(cudaEventSynchronize(ec));
             float t1 = 0, t2 = 0;
@@ -1883,6 +1986,10 @@ int gs_set_option(gs_ctx* ctx, int option, int value) {
             ctx->corr_tile = value;
             return GS_OK;
         case GS_OPT_AUTOTUNE: ctx->autotune = value != 0; return GS_OK;
+        case GS_OPT_ANGLES_PER_LAUNCH:
+            if (value < 0) return set_err(ctx, GS_ERR_ARG, "angles per launch must be >= 0");
+            ctx->angles_per_launch = value;
+            return GS_OK;
         default: return set_err(ctx, GS_ERR_ARG, "unknown option %d", option);
     }
 }
@@ -1907,7 +2014,7 @@ int gs_refine(gs_ctx* ctx, gs_refine_pick* picks, int n, int steps, gs_refine_re
 
 int gs_get_tuning(gs_ctx* ctx, int* out, int n) {
     if (!ctx || !out || n < 0) return set_err(ctx, GS_ERR_ARG, "null pointer or n < 0");
-    for (int i = 0; i < n && i < 5; ++i) out[i] = ctx->last_tuning[i];
+    for (int i = 0; i < n && i < 6; ++i) out[i] = ctx->last_tuning[i];
     return GS_OK;
 }
 

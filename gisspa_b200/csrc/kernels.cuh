@@ -413,15 +413,25 @@ __global__ void k_scale_images(float2* __restrict__ d, long long per_img, const 
 // squares of each template over the full l x l frame.
 // Reference: rotate_subIMG + apply_mask + compute_sum_sqr
 // (GPU_func.cu:496-560, 229-247, 363-407; main.cu:669-685).
+// Several angles in one launch: with `cs` set, blockIdx.z selects angle z of
+// the group ((cos, sin) = cs[z]), its images start at out + z Np l^2 and its
+// sums at stats + 2 z ntmpl; without it, (cose, sine) and one angle.
 __global__ void __launch_bounds__(256) k_pair_rotate(const float* __restrict__ tmpl, int ntmpl, int l, float cose,
-                                                     float sine, float d_m, float2* __restrict__ out,
-                                                     double* __restrict__ stats) {
+                                                     float sine, const float2* __restrict__ cs, float d_m,
+                                                     float2* __restrict__ out, double* __restrict__ stats) {
     __shared__ double red[4 * 32];
     const int p = blockIdx.y;
     const int J1 = 2 * p, J2 = 2 * p + 1;
     const bool has2 = J2 < ntmpl;
     const float* t1 = tmpl + (size_t)J1 * l * l;
     const float* t2 = tmpl + (size_t)(has2 ? J2 : J1) * l * l;
+    if (cs) {
+        const float2 c = cs[blockIdx.z];
+        cose = c.x;
+        sine = c.y;
+        out += (size_t)blockIdx.z * gridDim.y * l * l;
+        stats += (size_t)blockIdx.z * 2 * ntmpl;
+    }
     float2* o = out + (size_t)p * l * l;
     const int h = l / 2;
     const float dm = 1.5f * d_m;
@@ -474,10 +484,16 @@ __global__ void __launch_bounds__(256) k_pair_rotate(const float* __restrict__ t
 // Per-template (mean, 1/sd) over the full frame; mean subtraction skipped if
 // the mean is 0 and scaling skipped if the variance is 0, as in
 // substract_by_mean / divided_by_var (GPU_func.cu:424-443, main.cu:696-707).
-__global__ void k_pair_coef(const double* __restrict__ stats, int ntmpl, int l, float4* __restrict__ coef) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+// `nang` angles one after the other: pair p of angle z at coef[z Np + p],
+// from stats + 2 z ntmpl.
+__global__ void k_pair_coef(const double* __restrict__ stats, int ntmpl, int l, float4* __restrict__ coef,
+                            int nang) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int np = (ntmpl + 1) / 2;
-    if (p >= np) return;
+    if (i >= np * nang) return;
+    const int z = i / np, p = i - z * np;
+    stats += (size_t)z * 2 * ntmpl;
+    coef += (size_t)z * np;
     const double n = (double)l * l;
     float c[4] = {0.0f, 1.0f, 0.0f, 0.0f};
     for (int k = 0; k < 2; ++k) {

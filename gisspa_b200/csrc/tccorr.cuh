@@ -393,13 +393,13 @@ __global__ void __launch_bounds__(TcCfg<N2, kBf16>::kThreads, 1) k_corr_tc(CorrA
                     const int2 wp = a.unit_wp[u];
                     const UnitAcc* ac = a.acc + 2 * (long long)u;
                     for (int q = 0; q < 2; ++q) {
-                        const int J = 2 * wp.y + q;
-                        if (J >= a.ntmpl) break;
+                        const long long o = unit_out_index(wp.y, q, wp.x, a.pairs, a.ntmpl, a.out_stride);
+                        if (o < 0) break;
                         UnitAcc v;
                         v.key = __ldcg(&ac[q].key);
                         v.s1 = __ldcg(&ac[q].s1);
                         v.s2 = __ldcg(&ac[q].s2);
-                        a.out[(long long)wp.x * a.ntmpl + J] = unit_score(v, C::L);
+                        a.out[o] = unit_score(v, C::L);
                     }
                 }
             }

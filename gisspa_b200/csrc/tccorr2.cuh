@@ -41,22 +41,24 @@ namespace gs {
 
 struct Tc2Args {
     const float2* W;         // window spectra (PfaCols column order), Nw x L2
-    const float2* P;         // template-pair spectra of this angle (PfaCols order), Np x L2
+    const float2* P;         // template-pair spectra of the launch's angles (PfaCols order), (angles x pairs) x L2
     const __half2* W16;      // the same in FP16, row-tile order (k_to_half_tiles), scaled by s_w
     const __half2* P16;      // the same for the pairs, scaled by s_p
     __half2* R;              // scratch ring, S x L2 half2 (FP16 re, im in 8-column blocks)
     const float* wmax;       // per window max |W|
     const float* pmax;       // per pair max |P|
-    const int2* unit_wp;     // unit -> (window, pair)
+    const int2* unit_wp;     // unit -> (window, angle x pairs + pair)
     int* done_rows;          // per unit, row-tile warps finished
     int* done_cols;          // per unit, column-tile warps finished
     UnitAcc* acc;            // per unit, 2 templates (key, s2 of the scaled map)
-    UnitOut* out;            // this angle's results, index w * ntmpl + J
+    UnitOut* out;            // results, index angle * out_stride + w * ntmpl + J
     int* next_item;          // claim counter
     int* error;              // set when a bounded wait gives up
     int nu, ntmpl, S, lag;
     long long L2;
     int yb0, yb1;            // border interval of unshifted indices (both axes)
+    int pairs;               // template pairs per angle
+    long long out_stride;    // results per angle (windows x templates)
 };
 
 template <int kProducts_>
@@ -541,15 +543,15 @@ __device__ __forceinline__ void tc2_finish_unit(const Tc2Args& a, int u) {
                             l2 * ((double)w0.y * p0.x - (double)w0.x * p0.y)};
     const double inv = 1.0 / (double)s;
     for (int q = 0; q < 2; ++q) {
-        const int J = 2 * wp.y + q;
-        if (J >= a.ntmpl) break;
+        const long long o = unit_out_index(wp.y, q, wp.x, a.pairs, a.ntmpl, a.out_stride);
+        if (o < 0) break;
         UnitAcc v;
         v.key = __ldcg(&ac[q].key);
         v.s2 = __ldcg(&ac[q].s2) * inv * inv;
         // unscaled peak: the key's value is s x peak, exactly (s a power of two)
         const float pk = key_value(v.key) * (float)inv;
         v.key = v.key ? argmax_key(pk, key_index(v.key)) : 0ull;
-        a.out[(long long)wp.x * a.ntmpl + J] = unit_score(v, sums[q], C::L);
+        a.out[o] = unit_score(v, sums[q], C::L);
     }
 }
 

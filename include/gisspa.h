@@ -223,7 +223,8 @@ void gs_picks_free(gs_pick* picks);
  *  [4] row-pass kernel ms (sum)       [5] row-pass launches
  *  [6] column-pass kernel ms (sum)    [7] column-pass launches
  * With the persistent correlation kernel, [4]/[5] hold its time and launches
- * and [6]/[7] are zero.  Entries 4-7 are filled only while per-kernel timing
+ * (one launch covers gs_get_tuning's [5] angles, the last launch the
+ * remainder) and [6]/[7] are zero.  Entries 4-7 are filled only while per-kernel timing
  * is enabled. */
 #define GS_TIMING_COUNT 8
 int gs_get_timings(struct gs_ctx* ctx, float* out, int n);
@@ -290,8 +291,9 @@ int gs_merge_duplicates(int device, const gs_merge_item* items, size_t n, double
                         double euler_thres, unsigned char* keep);
 
 /* Scheduling the last search used for the persistent correlation (after
- * autotuning when GS_OPT_AUTOTUNE is on): the first min(n, 5) of {ring
- * slots, lag, window block, CTAs per SM (0 = as many as fit), tile width}. */
+ * autotuning when GS_OPT_AUTOTUNE is on): the first min(n, 6) of {ring
+ * slots, lag, window block, CTAs per SM (0 = as many as fit), tile width,
+ * in-plane angles per launch}. */
 int gs_get_tuning(struct gs_ctx* ctx, int* out, int n);
 
 /* Enable (1) or disable (0) per-kernel event timing of the correlation
@@ -334,6 +336,15 @@ int gs_set_kernel_timing(struct gs_ctx* ctx, int enable);
  * (256-thread CTAs, two per SM; default) or 8 (128-thread CTAs, four per
  * SM).  The autotuner also tries both. */
 #define GS_OPT_CORR_TILE 9
+/* GS_OPT_ANGLES_PER_LAUNCH: in-plane angles whose units one persistent
+ * correlation launch covers (their pair spectra are computed first, all
+ * resident at once).  0 (default) = enough angles for about 16384 (window,
+ * template pair) units per launch, with the pair spectra of one launch
+ * within 8 GiB; with GS_OPT_AUTOTUNE on, the autotuner then also times 1,
+ * a quarter, half and all of that count and keeps the fastest per angle.
+ * A count above the angle count is clamped, and so is one whose item
+ * indices would overflow. */
+#define GS_OPT_ANGLES_PER_LAUNCH 10
 int gs_set_option(struct gs_ctx* ctx, int option, int value);
 
 /* Counters of this context since creation (no reference counterpart; the
