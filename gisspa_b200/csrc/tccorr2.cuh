@@ -574,9 +574,9 @@ __device__ __forceinline__ const int* tc2_row_dep(const Tc2Args& a, int s) {
     return s >= a.S ? a.done_cols + (s - a.S) : nullptr;
 }
 
-// Count one finished tile (leader thread, after a release fence that orders
-// the pipeline's earlier stores and atomics before it); the last column tile
-// of a unit computes its scores.
+// Count one finished tile (one thread of the pipeline, after a release fence
+// that orders the pipeline's earlier stores and atomics before it); the last
+// column tile of a unit computes its scores.
 template <class C>
 __device__ __forceinline__ void tc2_publish(const Tc2Args& a, int item) {
     const int s = item / (2 * C::T), j = item - s * (2 * C::T);
@@ -624,7 +624,7 @@ __global__ void __launch_bounds__(Tc2Cfg<kProducts>::kThreads, 1) k_corr_tc2(Tc2
     const Tc2Masks ymask = tc2_row_masks<C>(w.wt, a.yb0, a.yb1);
     const int total = (a.nu + a.lag) * 2 * C::T;
     // The pipeline leader claims batches of kBatch consecutive items (one
-    // atomic per batch), the pipeline processes them in order and the leader
+    // atomic per batch), the pipeline processes them in order and one thread
     // publishes the whole batch after its last item (one release for all of
     // them, after the barrier that orders every warp's stores and
     // accumulator atomics before it).  Deferring within a batch cannot
@@ -671,7 +671,9 @@ __global__ void __launch_bounds__(Tc2Cfg<kProducts>::kThreads, 1) k_corr_tc2(Tc2
         if (last_of_batch) {
             // every warp's stores and atomics of the batch before the release
             tc2_sync(w.g);
-            if (w.wt == 0) {
+            // published by lane 0 of the pipeline's last warp, so that its
+            // fence and atomics overlap the leader's wait for the next item
+            if (w.wt == 96) {
                 // release: the batch's stores and atomics (ordered before by
                 // the barrier) before its counts
                 asm volatile("fence.acq_rel.gpu;" ::: "memory");
