@@ -619,7 +619,7 @@ def run_ours(args, rank, world, local_rank):
         angles_per_launch = na * args.steps / max(kn, 1)
         flops_launch = nw * nt * unit_flops(l) * angles_per_launch
         achieved = flops_launch / (avg_ms * 1e-3) / 1e12
-        wblk = 4
+        wblk = ctx.tuning()[2]   # windows per block of the unit order
         hbm_bytes = (npairs * math.ceil(nw / wblk) + nw) * l2 * 8.0 * angles_per_launch  # P once per window block, W once per angle
         kname = ("k_corr_persistent (row + column tiles of %g angle(s) per launch)" % angles_per_launch
                  if args.precision == "fp32" else

@@ -309,11 +309,13 @@ int gs_set_kernel_timing(struct gs_ctx* ctx, int enable);
  * specialised kernels exist (default). */
 #define GS_OPT_TWO_PASS 2
 /* GS_OPT_WINDOW_BLOCK: windows per block of the persistent launch's unit
- * order (reuse of window and pair spectra in L2); default 4. */
+ * order (reuse of window and pair spectra in L2); default 4 (8 for the FP32
+ * kernel at window 512). */
 #define GS_OPT_WINDOW_BLOCK 3
 /* GS_OPT_CORR_SLOTS / GS_OPT_CORR_LAG: scratch maps in the persistent
  * launch's ring (default 16) and how many units after its row tiles a unit's
- * column tiles are queued (default 6); slots must exceed lag.  The
+ * column tiles are queued (default 6); slots must exceed lag.  The FP32
+ * kernel at window 512 defaults to 32 slots and a lag of 10.  The
  * all-tensor-core modes keep more items in flight and default to 24 slots and
  * a lag of 12 unless either option was set; they need lag >= 1 and
  * slots >= lag + 2 (GS_ERR_UNSUPPORTED otherwise). */
@@ -334,7 +336,7 @@ int gs_set_kernel_timing(struct gs_ctx* ctx, int enable);
 #define GS_OPT_AUTOTUNE 8
 /* GS_OPT_CORR_TILE: vectors per tile of the FP32 persistent kernel: 16
  * (256-thread CTAs, two per SM; default) or 8 (128-thread CTAs, four per
- * SM).  The autotuner also tries both. */
+ * SM; default at window 512).  The autotuner also tries both. */
 #define GS_OPT_CORR_TILE 9
 /* GS_OPT_ANGLES_PER_LAUNCH: in-plane angles whose units one persistent
  * correlation launch covers (their pair spectra are computed first, all

@@ -89,7 +89,8 @@ def test_autotuned_equals_default(data):
     with G.Context(0) as ctx:
         ctx.set_templates(_params(), tmpl, ctf)
         ref = ctx.search(img, ctf)
-        assert ctx.tuning() == (16, 6, 4, 0, 16)
+        # window 512, FP32: 32 ring slots, lag 10, window block 8, 8-vector tiles
+        assert ctx.tuning() == (32, 10, 8, 0, 8)
     with G.Context(0) as ctx:
         ctx.set_autotune(True)
         ctx.set_templates(_params(), tmpl, ctf)
