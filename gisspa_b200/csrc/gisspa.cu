@@ -52,6 +52,8 @@ namespace {
 struct gs_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;    // second stream: pair spectra while micrographs are prepared
+    cudaEvent_t side_ev[2] = {nullptr, nullptr};  // search start on `stream`; pair spectra done on `side`
     std::string err;
     std::map<int, FftPlan> plans;
     // templates
@@ -857,8 +859,14 @@ int gs_ctx_create(int device, gs_ctx** out) {
     if (device < 0 || device >= ndev) return GS_ERR_ARG;
     gs_ctx* ctx = new gs_ctx();
     ctx->device = device;
-    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->side_ev[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->side_ev[1], cudaEventDisableTiming) != cudaSuccess) {
         cudaGetLastError();
+        if (ctx->side_ev[0]) cudaEventDestroy(ctx->side_ev[0]);
+        if (ctx->side) cudaStreamDestroy(ctx->side);
+        if (ctx->stream) cudaStreamDestroy(ctx->stream);
         delete ctx;
         return GS_ERR_CUDA;
     }
@@ -870,6 +878,7 @@ int gs_ctx_destroy(gs_ctx* ctx) {
     if (!ctx) return GS_ERR_ARG;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    cudaStreamSynchronize(ctx->side);
     for (auto& kv : ctx->plans) cudaFree(kv.second.tw);
     DBuf* bufs[] = {&ctx->tmpl, &ctx->in, &ctx->q, &ctx->cimg, &ctx->img, &ctx->stats, &ctx->ra, &ctx->rb,
                     &ctx->off, &ctx->win, &ctx->wsum, &ctx->winv, &ctx->tspec, &ctx->scratch, &ctx->pstats,
@@ -880,6 +889,8 @@ int gs_ctx_destroy(gs_ctx* ctx) {
                     &ctx->tc2_pmax, &ctx->tc2_w16, &ctx->tc2_p16, &ctx->rot_cs};
     for (DBuf* b : bufs) free_buf(*b);
     for (cudaEvent_t e : ctx->kev) cudaEventDestroy(e);
+    for (cudaEvent_t e : ctx->side_ev) cudaEventDestroy(e);
+    cudaStreamDestroy(ctx->side);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return GS_OK;
@@ -1290,12 +1301,95 @@ static int autotune(gs_ctx* ctx, const float2* W, const float2* TS, int NW, Corr
     return GS_OK;
 }
 
+// Item indices of one persistent launch over n units (2 x l/8 tiles per
+// unit) must fit an int.
+static bool units_fit(int l, long long n) { return (n + 64) * 2 * (l / 8) < (1ll << 31); }
+
+// In-plane angles per persistent launch before any tuning: the option's
+// count, else enough angles for about kUnitsPerLaunch units (a launch's
+// ramp-up and drain, and the per-launch overhead, then weigh little against
+// its work) with the pair spectra of one launch within kAngleBudget bytes;
+// at most na, and within the item-index limit.
+static int launch_angles(const gs_ctx* ctx, int nu, int na, bool tc2) {
+    constexpr long long kUnitsPerLaunch = 16384;
+    constexpr double kAngleBudget = 8.0 * (1ull << 30);
+    const int l = ctx->l, Np = (ctx->ntmpl + 1) / 2;
+    const long long l2 = (long long)l * l;
+    const double angle_bytes = (double)sizeof(float2) * l2 * Np +
+                               (tc2 ? (double)sizeof(__half2) * l * 768 * Np + sizeof(float) * Np : 0.0);
+    int A;
+    if (ctx->angles_per_launch > 0) {
+        A = ctx->angles_per_launch;
+    } else {
+        A = (int)std::max(1ll, kUnitsPerLaunch / nu);
+        A = (int)std::min<double>(A, std::max(1.0, std::floor(kAngleBudget / angle_bytes)));
+    }
+    A = std::max(1, std::min(A, na));
+    while (A > 1 && !units_fit(l, (long long)A * nu)) --A;
+    return A;
+}
+
+// Every angle's (cos, sin) on the device, for the pair spectra of a group of
+// angles in one pass (synchronous: before any capture).
+static int upload_rotations(gs_ctx* ctx, const std::vector<float>& angles) {
+    const int na = (int)angles.size();
+    std::vector<float2> cs(std::max(1, na));
+    for (int i = 0; i < na; ++i) cs[i] = rotation_cs(angles[i]);
+    TRY(ensure(ctx, ctx->rot_cs, sizeof(float2) * cs.size()));
+    CK(cudaMemcpy(ctx->rot_cs.p, cs.data(), sizeof(float2) * na, cudaMemcpyHostToDevice));
+    return GS_OK;
+}
+
+// The first persistent launch's pair spectra, enqueued on the side stream
+// so that they overlap the micrograph preparation that follows on the main
+// stream (its exact-order statistics keep one SM busy for milliseconds).
+// *count = angles prefetched, 0 when the correlation tunes first (the tuner
+// times its own pair spectra), has no persistent launch, or norm_type 1.
+// side_ev[1] marks their completion.
+static int prefetch_pair_spectra(gs_ctx* ctx, int NW, const std::vector<float>& angles, int* count) {
+    *count = 0;
+    const gs_params& p = ctx->p;
+    const int l = ctx->l, N = ctx->ntmpl, Np = (N + 1) / 2, na = (int)angles.size();
+    const long long l2 = (long long)l * l;
+    const bool tc2 = p.precision == GS_PREC_TC_FULL || p.precision == GS_PREC_TC_FULL_1P;
+    const bool persistent = fast_ok(ctx, l) && !ctx->two_pass;
+    if (!persistent || ctx->autotune || p.norm_type == 1 || na == 0 || (tc2 && l != 720)) return GS_OK;
+    const int nu = Np * NW;
+    if (!units_fit(l, nu)) return GS_OK;  // the correlation reports it
+    const bool pfa = (p.precision == GS_PREC_FP32 || tc2) && PfaCols::make(l).N2 != 0;
+    const int A = launch_angles(ctx, nu, na, tc2);
+    TRY(ensure(ctx, ctx->tspec, sizeof(float2) * l2 * Np * A));
+    TRY(ensure(ctx, ctx->pstats, sizeof(double) * 2 * N * A));
+    TRY(ensure(ctx, ctx->coef, sizeof(float4) * Np * A));
+    TRY(upload_rotations(ctx, angles));
+    FftPlan* plan = nullptr;
+    TRY(get_plan(ctx, l, &plan));  // created (synchronously) before the side work
+    // after everything already on the main stream (an earlier search's
+    // correlation still reading the pair spectra)
+    CK(cudaEventRecord(ctx->side_ev[0], ctx->stream));
+    CK(cudaStreamWaitEvent(ctx->side, ctx->side_ev[0], 0));
+    // the launch helpers enqueue on ctx->stream: point it at the side stream
+    std::swap(ctx->stream, ctx->side);
+    int st = GS_OK;
+    constexpr int kImgs = 32768;
+    const int per = std::max(1, kImgs / Np);
+    float2* TS = P<float2>(ctx->tspec);
+    for (int k = 0; k < A && st == GS_OK; k += per)
+        st = pair_spectra_n(ctx, angles[k], P<float2>(ctx->rot_cs) + k, std::min(per, A - k),
+                            TS + (size_t)k * Np * l2, pfa);
+    std::swap(ctx->stream, ctx->side);
+    if (st != GS_OK) return st;
+    CK(cudaEventRecord(ctx->side_ev[1], ctx->side));
+    *count = A;
+    return GS_OK;
+}
+
 // Correlation of every window with every template over all angles (the
 // angle loop of main.cu:1232-1257): per angle the template-pair spectra, then
 // either one persistent launch over all (window, pair) units or per-window
 // row and column launches.  Results to ctx->units [angle][NW][N].
 static int correlate_all(gs_ctx* ctx, float2* W, int NW, const std::vector<float>& angles, float* t_spec,
-                         float* t_corr, float kt[4]) {
+                         float* t_corr, float kt[4], int prefetched = 0) {
     const gs_params& p = ctx->p;
     const int l = ctx->l;
     const long long l2 = (long long)l * l;
@@ -1313,41 +1407,21 @@ static int correlate_all(gs_ctx* ctx, float2* W, int NW, const std::vector<float
         return set_err(ctx, GS_ERR_UNSUPPORTED,
                        "tensor-core precision needs window 512, 720 or 768 and the persistent path (window %d)", l);
     const int nu = Np * NW;
-    // item indices of one launch (2 x l/8 tiles per unit) must fit an int
-    auto units_fit = [&](long long n) { return (n + 64) * 2 * (l / 8) < (1ll << 31); };
-    if (!units_fit(nu))
+    if (!units_fit(l, nu))
         return set_err(ctx, GS_ERR_UNSUPPORTED, "too many (window, template pair) units in one search (%d)", nu);
-    // In-plane angles per persistent launch: by default enough angles for
-    // about kUnitsPerLaunch units (a launch's ramp-up and drain, and the
-    // per-launch overhead, then weigh little against its work), with the
-    // pair spectra of all of them within kAngleBudget bytes; the option
-    // overrides the count, the item-index limit still applies.
-    constexpr long long kUnitsPerLaunch = 16384;
-    constexpr double kAngleBudget = 8.0 * (1ull << 30);
-    const double angle_bytes = (double)sizeof(float2) * l2 * Np +
-                               (tc2 ? (double)sizeof(__half2) * l * 768 * Np + sizeof(float) * Np : 0.0);
-    int A = 1;
-    if (persistent) {
-        if (ctx->angles_per_launch > 0) {
-            A = ctx->angles_per_launch;
-        } else {
-            A = (int)std::max(1ll, kUnitsPerLaunch / nu);
-            A = (int)std::min<double>(A, std::max(1.0, std::floor(kAngleBudget / angle_bytes)));
-        }
-        A = std::max(1, std::min(A, na));
-        while (A > 1 && !units_fit((long long)A * nu)) --A;
+    int A = persistent ? launch_angles(ctx, nu, na, tc2) : 1;
+    // pair spectra of the first launch already enqueued on the side stream
+    // (prefetch_pair_spectra): used when the group matches, else awaited
+    // and recomputed
+    if (prefetched && prefetched != A) {
+        CK(cudaStreamWaitEvent(ctx->stream, ctx->side_ev[1], 0));
+        prefetched = 0;
     }
     TRY(ensure(ctx, ctx->tspec, sizeof(float2) * l2 * Np * A));
     TRY(ensure(ctx, ctx->pstats, sizeof(double) * 2 * N * A));
     TRY(ensure(ctx, ctx->coef, sizeof(float4) * Np * A));
-    // every angle's (cos, sin) on the device, for the pair spectra of a group
-    // of angles in one pass (uploaded before any capture)
-    {
-        std::vector<float2> cs(na);
-        for (int i = 0; i < na; ++i) cs[i] = rotation_cs(angles[i]);
-        TRY(ensure(ctx, ctx->rot_cs, sizeof(float2) * std::max(1, na)));
-        CK(cudaMemcpy(ctx->rot_cs.p, cs.data(), sizeof(float2) * na, cudaMemcpyHostToDevice));
-    }
+    // (a prefetch uploaded them already, and its kernels may still read them)
+    if (!prefetched) TRY(upload_rotations(ctx, angles));
     TRY(ensure(ctx, ctx->acc, sizeof(UnitAcc) * N));
     TRY(ensure(ctx, ctx->units, sizeof(UnitOut) * std::max<long long>(1, total_units)));
     float2* TS = P<float2>(ctx->tspec);
@@ -1458,15 +1532,20 @@ static int correlate_all(gs_ctx* ctx, float2* W, int NW, const std::vector<float
     float k1ms = 0, k2ms = 0;
     long long k1n = 0, k2n = 0;
 
+    bool capturing = false;  // enqueue_group is being captured into the graph
     // the work of angles a0 .. a0 + ag - 1 (ag = 1 without the persistent
     // kernel), enqueued on the context's stream: their pair spectra one
     // after the other in TS, then one correlation launch over all their units
     auto enqueue_group = [&](int a0, int ag, bool rec) -> int {
         if (rec) CK(cudaEventRecord(ea, ctx->stream));
-        // pair spectra of the group, in passes of at most kImgs images
+        // pair spectra of the group, in passes of at most kImgs images (the
+        // first group's may come from the side stream: in the stream loop
+        // the main stream waits for them here, a graph waits before capture)
         constexpr int kImgs = 32768;
         const int per = std::max(1, kImgs / Np);
-        for (int k = 0; k < ag; k += per) {
+        const bool have = prefetched && a0 == 0;
+        if (have && !capturing) CK(cudaStreamWaitEvent(ctx->stream, ctx->side_ev[1], 0));
+        for (int k = 0; k < ag && !have; k += per) {
             const int n = std::min(per, ag - k);
             TRY(pair_spectra_n(ctx, angles[a0 + k], P<float2>(ctx->rot_cs) + a0 + k, n,
                                TS + (size_t)k * Np * l2, pfa));
@@ -1556,10 +1635,13 @@ static int correlate_all(gs_ctx* ctx, float2* W, int NW, const std::vector<float
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
         const unsigned long long launches0 = ctx->counters.kernel_launches;
+        if (prefetched) CK(cudaStreamWaitEvent(ctx->stream, ctx->side_ev[1], 0));
+        capturing = true;
         CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
         int st = GS_OK;
         for (int ai = 0; ai < na && st == GS_OK; ai += A) st = enqueue_group(ai, std::min(A, na - ai), false);
         const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
+        capturing = false;
         if (st != GS_OK) {
             if (graph) cudaGraphDestroy(graph);
             return st;
@@ -1695,6 +1777,16 @@ static int search_many(gs_ctx* ctx, std::vector<MicPlan>& mics, std::vector<std:
     for (auto& e : ev) CK(cudaEventCreate(&e));
     struct EvGuard { cudaEvent_t* e; ~EvGuard() { for (int i = 0; i < 4; ++i) cudaEventDestroy(e[i]); } } evg{ev};
     CK(cudaEventRecord(ev[0], ctx->stream));
+    // the first launch's pair spectra on the side stream during the
+    // micrograph preparation; whatever path the search takes, the main
+    // stream's later work is ordered after them
+    int prefetched = 0;
+    TRY(prefetch_pair_spectra(ctx, NW, angles, &prefetched));
+    struct SideJoin {
+        gs_ctx* ctx;
+        const int* on;
+        ~SideJoin() { if (*on) cudaStreamWaitEvent(ctx->stream, ctx->side_ev[1], 0); }
+    } side_join{ctx, &prefetched};
     TRY(ensure(ctx, ctx->win, sizeof(float2) * l2 * NW));
     float2* W = P<float2>(ctx->win);
     for (const MicPlan& mp : mics) TRY(prep_micrograph(ctx, mp, W));
@@ -1711,7 +1803,7 @@ static int search_many(gs_ctx* ctx, std::vector<MicPlan>& mics, std::vector<std:
         const MicPlan& mp = mics[0];
         TRY(search_norm1(ctx, W, mp.nx, mp.ny, mp.offx, mp.offy, angles, &t_spec, &t_corr, &(*res)[0]));
     } else {
-        TRY(correlate_all(ctx, W, NW, angles, &t_spec, &t_corr, kt));
+        TRY(correlate_all(ctx, W, NW, angles, &t_spec, &t_corr, kt, prefetched));
         ctx->last_na = na;
         ctx->last_nw = NW;
         ctx->last_nt = N;
