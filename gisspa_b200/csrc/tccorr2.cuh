@@ -200,8 +200,10 @@ __device__ __forceinline__ void tc2_wait_counter(const int* p, int target, int* 
     atomicExch(error, 1);
 }
 
-// Issue a GEMM stage (thread 0 of the pipeline), commit, wait for it (one
-// lane per warp polls the mbarrier).  Returns false when the bounded wait gave up.
+// Issue a GEMM stage (thread 0 of the pipeline), commit, wait for it (lane
+// 0 of every warp waits on the mbarrier itself, so the warps resume as soon
+// as the MMAs complete, without a pipeline barrier).  Returns false when this
+// warp's bounded wait gave up.
 template <class C, bool kStage2, bool kColPass>
 __device__ __forceinline__ bool tc2_gemm(const Tc2Wg& w, unsigned char* sm, uint32_t& phase, int* a_error,
                                          const int* dep = nullptr) {
@@ -240,12 +242,12 @@ __device__ __forceinline__ bool tc2_gemm(const Tc2Wg& w, unsigned char* sm, uint
                                     (j | p) ? 1u : 0u);
         }
         tc::mma_commit(w.bar);
-        // a dependency to check after the MMAs: its acquire load is issued
-        // now, so that its round trip overlaps them
+    }
+    // every warp waits for the MMAs itself (its lane 0, sleeping between
+    // polls; bounded: 2 s, or 1 ms once any wait of the launch has given up)
+    // and checks the dependency, so that no pipeline barrier follows
+    if ((w.wt & 31) == 0) {
         const int dv = dep ? ld_acquire_gpu(dep) : C::kDone;
-        // the issuing thread alone waits (sleeping between polls; bounded:
-        // 2 s, or 1 ms once any wait of the launch has given up); the other
-        // warps block on the barrier below and take no issue slots
         const uint64_t limit = *(volatile const int*)a_error ? 1000000ull : 2000000000ull;
         if (!tc::mbar_wait_backoff(w.bar, phase, limit)) {
             ok = 0;
@@ -254,9 +256,7 @@ __device__ __forceinline__ bool tc2_gemm(const Tc2Wg& w, unsigned char* sm, uint
         if (dv < C::kDone) tc2_wait_counter<C>(dep, C::kDone, a_error);
     }
     phase ^= 1u;
-    // the MMAs' completion, observed by the issuing thread, ordered before
-    // every thread's TMEM reads and operand rewrites
-    tc2_sync(w.g);
+    __syncwarp();
     tc::fence_after_sync();
     return ok != 0;
 }
