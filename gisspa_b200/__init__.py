@@ -30,6 +30,9 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "out of memory", 3: "CUDA error",
           7: "I/O error"}
 # arithmetic of the correlation's DFT stages (gs_params.precision)
 GS_PREC_FP32, GS_PREC_TC_BF16, GS_PREC_TC_FP16, GS_PREC_TC_FULL, GS_PREC_TC_FULL_1P = 0, 1, 2, 3, 4
+# gs_set_option options (include/gisspa.h)
+GS_OPT_GENERIC_FFT, GS_OPT_TWO_PASS, GS_OPT_WINDOW_BLOCK, GS_OPT_CORR_SLOTS, GS_OPT_CORR_LAG = 1, 2, 3, 4, 5
+GS_OPT_CORR_CTAS, GS_OPT_GRAPH, GS_OPT_AUTOTUNE, GS_OPT_CORR_TILE, GS_OPT_ANGLES_PER_LAUNCH = 6, 7, 8, 9, 10
 
 
 class GsParams(C.Structure):
@@ -376,15 +379,15 @@ class Context:
 
     def set_graph(self, enable: bool) -> None:
         """Capture the angle loop as one CUDA graph (GS_OPT_GRAPH)."""
-        self._check(self._lib.gs_set_option(self._h, 7, 1 if enable else 0), "gs_set_option")
+        self._check(self._lib.gs_set_option(self._h, GS_OPT_GRAPH, 1 if enable else 0), "gs_set_option")
 
     def set_autotune(self, enable: bool) -> None:
         """Tune the persistent kernel's scheduling on first use (GS_OPT_AUTOTUNE)."""
-        self._check(self._lib.gs_set_option(self._h, 8, 1 if enable else 0), "gs_set_option")
+        self._check(self._lib.gs_set_option(self._h, GS_OPT_AUTOTUNE, 1 if enable else 0), "gs_set_option")
 
     def set_corr_ctas(self, per_sm: int) -> None:
         """Resident CTAs per SM of the persistent kernel (0 = as many as fit)."""
-        self._check(self._lib.gs_set_option(self._h, 6, int(per_sm)), "gs_set_option")
+        self._check(self._lib.gs_set_option(self._h, GS_OPT_CORR_CTAS, int(per_sm)), "gs_set_option")
 
     def tuning(self) -> Tuple[int, int, int, int, int]:
         """(ring slots, lag, window block, CTAs per SM, tile width) of the last search."""
@@ -395,7 +398,7 @@ class Context:
     def set_angles_per_launch(self, angles: int) -> None:
         """In-plane angles per persistent correlation launch (GS_OPT_ANGLES_PER_LAUNCH;
         0 = chosen from the unit count)."""
-        self._check(self._lib.gs_set_option(self._h, 10, int(angles)), "gs_set_option")
+        self._check(self._lib.gs_set_option(self._h, GS_OPT_ANGLES_PER_LAUNCH, int(angles)), "gs_set_option")
 
     def angles_per_launch(self) -> int:
         """In-plane angles per persistent launch of the last search."""
@@ -405,7 +408,7 @@ class Context:
 
     def set_corr_tile(self, vectors: int) -> None:
         """Tile width of the FP32 persistent kernel (16 or 8 vectors)."""
-        self._check(self._lib.gs_set_option(self._h, 9, int(vectors)), "gs_set_option")
+        self._check(self._lib.gs_set_option(self._h, GS_OPT_CORR_TILE, int(vectors)), "gs_set_option")
 
     def search_device(self, dev_ptr: int, nx: int, ny: int, ctf) -> np.ndarray:
         ptr = C.POINTER(GsPick)()
@@ -451,26 +454,26 @@ class Context:
 
     def set_generic_fft(self, enable: bool) -> None:
         """Force the generic mixed-radix kernels (cross-check of the fast path)."""
-        self._check(self._lib.gs_set_option(self._h, 1, 1 if enable else 0), "gs_set_option")
+        self._check(self._lib.gs_set_option(self._h, GS_OPT_GENERIC_FFT, 1 if enable else 0), "gs_set_option")
 
     def set_two_pass(self, enable: bool) -> None:
         """Run the correlation as per-window row and column launches instead of
         one persistent launch per angle (cross-check of the persistent kernel)."""
-        self._check(self._lib.gs_set_option(self._h, 2, 1 if enable else 0), "gs_set_option")
+        self._check(self._lib.gs_set_option(self._h, GS_OPT_TWO_PASS, 1 if enable else 0), "gs_set_option")
 
     def set_window_block(self, windows: int) -> None:
         """Windows per block of the persistent kernel's unit order."""
-        self._check(self._lib.gs_set_option(self._h, 3, int(windows)), "gs_set_option")
+        self._check(self._lib.gs_set_option(self._h, GS_OPT_WINDOW_BLOCK, int(windows)), "gs_set_option")
 
     def set_corr_ring(self, slots: int, lag: int) -> None:
         """Scratch-map ring size and column-tile lag of the persistent kernel."""
         # order matters: each call checks slots > lag against the current other value
         if slots > self._lag_now():
-            self._check(self._lib.gs_set_option(self._h, 4, int(slots)), "gs_set_option")
-            self._check(self._lib.gs_set_option(self._h, 5, int(lag)), "gs_set_option")
+            self._check(self._lib.gs_set_option(self._h, GS_OPT_CORR_SLOTS, int(slots)), "gs_set_option")
+            self._check(self._lib.gs_set_option(self._h, GS_OPT_CORR_LAG, int(lag)), "gs_set_option")
         else:
-            self._check(self._lib.gs_set_option(self._h, 5, int(lag)), "gs_set_option")
-            self._check(self._lib.gs_set_option(self._h, 4, int(slots)), "gs_set_option")
+            self._check(self._lib.gs_set_option(self._h, GS_OPT_CORR_LAG, int(lag)), "gs_set_option")
+            self._check(self._lib.gs_set_option(self._h, GS_OPT_CORR_SLOTS, int(slots)), "gs_set_option")
         self._lag = int(lag)
 
     def _lag_now(self) -> int:

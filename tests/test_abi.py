@@ -20,6 +20,16 @@ def test_header_matches_python_binding():
     assert sorted(G.EXPORTS) == _declared()
 
 
+def test_header_constants_match_python_binding():
+    """Every GS_OPT_* and GS_PREC_* value the header defines is the Python
+    module's constant of the same name."""
+    src = open(os.path.join(ROOT, "include", "gisspa.h")).read()
+    defs = dict(re.findall(r"^#define (GS_(?:OPT|PREC)_[A-Z0-9_]+) (\d+)\s*$", src, flags=re.M))
+    assert len(defs) >= 15, defs
+    for name, value in defs.items():
+        assert getattr(G, name) == int(value), name
+
+
 def test_library_exports_every_declared_symbol():
     if not os.path.exists(G.LIB_PATH):
         from gisspa_b200 import build
