@@ -1378,8 +1378,12 @@ static int prefetch_pair_spectra(gs_ctx* ctx, int NW, const std::vector<float>& 
         st = pair_spectra_n(ctx, angles[k], P<float2>(ctx->rot_cs) + k, std::min(per, A - k),
                             TS + (size_t)k * Np * l2, pfa);
     std::swap(ctx->stream, ctx->side);
-    if (st != GS_OK) return st;
     CK(cudaEventRecord(ctx->side_ev[1], ctx->side));
+    if (st != GS_OK) {
+        // whatever was enqueued stays ordered before the main stream's later work
+        cudaStreamWaitEvent(ctx->stream, ctx->side_ev[1], 0);
+        return st;
+    }
     *count = A;
     return GS_OK;
 }
