@@ -287,6 +287,26 @@ DTYPES = {"fp32": "f32", "tc-bf16": "bf16 hi+lo split, f32 accumulate",
 TRAFFIC_PER_PAIR_UNIT_L720 = (10585217280 + 106544128) / 8800.0
 
 
+def compare_picks(base, other, thres: float) -> dict:
+    """Picks of another path against the base path's.  A pick is an (angle,
+    window, template) unit at or above the threshold; the pick sets must be
+    equal except units whose score lies within 1e-3 (relative) of the
+    threshold, the scores of common units are compared relatively, and a
+    common unit whose peak position differs counts as moved."""
+    key = lambda p: (int(p["angle_index"]), int(p["window_x"]), int(p["window_y"]), int(p["template_index"]))
+    b = {key(p): float(p["score"]) for p in base}
+    o = {key(p): float(p["score"]) for p in other}
+    bc = {key(p): (float(p["center_x"]), float(p["center_y"])) for p in base}
+    oc = {key(p): (float(p["center_x"]), float(p["center_y"])) for p in other}
+    common = set(b) & set(o)
+    only = set(b) ^ set(o)
+    sc = [b.get(k, o.get(k)) for k in only]
+    return {"picks": [len(b), len(o)], "equal_picks": not only, "picks_differing": len(only),
+            "differing_picks_within_1e-3_of_threshold": all(abs(x - thres) <= 1e-3 * abs(thres) for x in sc),
+            "max_rel_score_diff": max([abs(b[k] - o[k]) / abs(b[k]) for k in common], default=0.0),
+            "peaks_moved": sum(bc[k] != oc[k] for k in common)}
+
+
 def tensor_core_comparison(ds, kw, local_rank, base_precision: str):
     """The correlation paths on the same micrograph and templates over three
     in-plane angles (0, 120, 240 deg): per-angle correlation time of the FP32
@@ -325,28 +345,13 @@ def tensor_core_comparison(ds, kw, local_rank, base_precision: str):
         r["micrographs_per_s_at_72_angles"] = 1000.0 / (r["micrograph_prep_plus_spectra_per_angle_ms"]
                                                         + 72 * r["per_angle_correlation_ms"])
         res[name] = r
-    # a pick is a (angle, window, template) unit at or above the threshold; its
-    # peak may move between near-equal pixels (counted separately)
-    key = lambda p: (int(p["angle_index"]), int(p["window_x"]), int(p["window_y"]), int(p["template_index"]))
     out = {"angles_timed": 3, "note": "same micrograph and templates as the headline; per-angle times "
            "extrapolated to 72 angles for the micrographs/s of each path", "threshold": thres}
-    base = {key(p): float(p["score"]) for p in picks.get("fp32", [])}
-    base_c = {key(p): (float(p["center_x"]), float(p["center_y"])) for p in picks.get("fp32", [])}
     for name in names:
         r = dict(res[name])
         if name != "fp32" and "error" not in r and "fp32" in picks:
-            other = {key(p): float(p["score"]) for p in picks[name]}
-            other_c = {key(p): (float(p["center_x"]), float(p["center_y"])) for p in picks[name]}
-            common = set(base) & set(other)
-            only = set(base) ^ set(other)
-            sc = [base.get(k, other.get(k)) for k in only]
             r["speed_over_fp32"] = res["fp32"]["per_angle_correlation_ms"] / r["per_angle_correlation_ms"]
-            r["picks"] = [len(base), len(other)]
-            r["equal_picks"] = not only
-            r["picks_differing"] = len(only)
-            r["differing_picks_within_1e-3_of_threshold"] = all(abs(x - thres) <= 1e-3 * abs(thres) for x in sc)
-            r["max_rel_score_diff"] = max([abs(base[k] - other[k]) / abs(base[k]) for k in common], default=0.0)
-            r["peaks_moved"] = sum(base_c[k] != other_c[k] for k in common)
+            r.update(compare_picks(picks["fp32"], picks[name], thres))
         out[name.replace("-", "_")] = r
     done = [n for n in names[1:] if "speed_over_fp32" in out[n.replace("-", "_")]]
     if done:
